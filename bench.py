@@ -1,0 +1,335 @@
+#!/usr/bin/env python
+"""Benchmark: points*steps/s of the four-level interferogram sweep on B200.
+
+Workload (the configuration the headline metric is quoted on): N = 4 Lindblad model, 2048 x 2048
+grid of (eps, A), RK4 with 8000 steps over t in [0, 400], time-averaged <|3><3|> map. One bench
+"step" is one full sweep of that grid. The headline ``value`` is the FP32 form (FP32 state and
+RHS, FP64 time / drive phase / compensated average) with device-resident inputs; the plain FP64
+form is timed beside it on the same GPU and the FP32 map's max-abs error against it is reported.
+
+Multi-GPU (torchrun): weak scaling - rank r sweeps its own 2048 x 2048 tile (rows r*2048 ..
+of a (2048 N) x 2048 grid); no collective on the data path, timings are the max over ranks.
+
+``--impl reference`` times the reference's own kernel code on the host CPU cores (the CUDA
+source that GQIS generates for this model, compiled for the CPU with OpenMP; falls back to
+the NumPy oracle) on a strided sample of the same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "gpu-quantum-interferometry-solver_b200"))
+
+METRIC = "points*steps/s (RK4, four-level Lindblad sweep); FP32 form vs plain FP64 at <=1e-6 max-abs err"
+UNIT = "points*steps/s"
+SIDE, NSTEPS, DURATION = 2048, 8000, 400.0
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index, self.proc, self.lines = index, None, []
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.index), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _flush_l2(torch, buf):
+    buf.add_(1)  # 256 MiB write: larger than the 126 MB L2
+
+
+def time_launches(torch, sweep, steps, warmup, flush):
+    """Per-launch CUDA-event times (ms) of ``steps`` launches after ``warmup`` launches."""
+    stream = torch.cuda.current_stream()
+    for _ in range(warmup):
+        sweep.launch(stream)
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(steps):
+        _flush_l2(torch, flush)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        sweep.launch(stream)
+        b.record(stream)
+        b.synchronize()
+        times.append(a.elapsed_time(b))
+    return times
+
+
+def _max_over_ranks(torch, value, ws):
+    if ws <= 1:
+        return value
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_reference(steps=1, sample="c2_fp64_mean_sub64"):
+    """Reference kernel (GQIS-generated CUDA source compiled for the CPU) on host cores."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import ref_kernels
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    if ref_kernels.available(sample, "cpu"):
+        meta = ref_kernels.meta(sample)
+        shape = meta["outputs"][0]["shape"]
+        points = shape[0] * shape[1]
+        nsteps = [a for a in meta["args"] if a["kind"] == "scalar"][4]["value"]
+        times = []
+        for _ in range(steps):
+            _, dt = ref_kernels.run_case(sample, "cpu")
+            times.append(dt)
+        return {"kind": "reference", "points": points, "steps": nsteps, "times": times, "cores": cores,
+                "sample": f"{shape[0]}x{shape[1]} strided subgrid of the 2048x2048 grid, {nsteps} RK4 steps, "
+                          "reference GQIS FP64 kernel source compiled for the CPU (OpenMP)"}
+    import numpy as np
+    import lindblad_oracle
+    sys.path.insert(0, str(ROOT / "gpu-quantum-interferometry-solver_b200"))
+    from gqis import workloads
+    w = workloads.four_level(side=16, steps=800, duration=40.0)
+    model = lindblad_oracle.from_workload(w)
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        lindblad_oracle.rk4_sweep(model, w["tlist"])
+        times.append(time.perf_counter() - t0)
+    return {"kind": "port", "points": 256, "steps": 800, "times": times, "cores": 1,
+            "sample": "16x16 strided subgrid, 800 RK4 steps, NumPy density-matrix oracle (one core)"}
+
+
+def run_reference(args):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    ref = cpu_reference(steps=args.warmup + args.steps)
+    times = ref["times"][args.warmup:]
+    per = [ref["points"] * ref["steps"] / t for t in times]
+    value = statistics.median(per)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.median(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": f"four-level Lindblad RK4 sweep, {ref['sample']}"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": ref["cores"], "kind": ref["kind"],
+                             "sample": ref["sample"]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def _traffic_from_profiles():
+    p = ROOT / "profiles" / "roofline_inputs.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text())
+        except ValueError:
+            return {}
+    return {}
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    ws, rank, local = _dist()
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    import gqis
+    from gqis import native, solver, workloads
+
+    side, nsteps = args.side, args.nsteps
+    w = workloads.four_level(side=None, steps=nsteps, duration=DURATION * nsteps / NSTEPS, full=side * ws)
+    eps, A = w["symbols"]
+    eps_axis = w["var_arrays"][eps][rank * side:(rank + 1) * side]
+    a_axis = np.linspace(0.0, 5.0, side)
+    call = dict(var_arrays={eps: eps_axis, A: a_axis}, const_values={})
+    model = (w["H"], w["Drive"], w["Col_Ops"], w["mean_operator"], w["tlist"])
+    fp32 = solver.prepare_sweep("mesolve_2D", *model, **call, precision="fp32")
+    fp64 = solver.prepare_sweep("mesolve_2D", *model, **call, precision="fp64")
+    flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    points, ksteps = fp32.points, fp32.steps
+
+    peaks = {}
+    if rank == 0:
+        for kind, name in ((0, "fp64"), (1, "fp32"), (2, "fp32x2")):
+            peaks[name] = native.probe_fma_tflops(kind)
+
+    # ---- plain FP64 (timed first, its map is the accuracy reference of the FP32 form)
+    _barrier(ws)
+    t64 = time_launches(torch, fp64, args.steps, args.warmup, flush)
+    ms64 = _max_over_ranks(torch, float(np.mean(t64)), ws)
+    ref_map = fp64.results.clone()
+
+    # ---- headline: FP32 form
+    _barrier(ws)
+    sampler = ClockSampler(local).start()
+    torch.cuda.synchronize()
+    t32 = time_launches(torch, fp32, args.steps, args.warmup, flush)
+    clocks = sampler.stop()
+    ms32 = _max_over_ranks(torch, float(np.mean(t32)), ws)
+    err = float((fp32.results.double() - ref_map).abs().max().item())
+    err = _max_over_ranks(torch, err, ws)
+
+    # ---- end to end through the public API (host arrays in, NumPy map out)
+    e2e_ms = []
+    for k in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        out = gqis.mesolve_2D(*model, **call, fp64=False)
+        b.record()
+        b.synchronize()
+        if k >= args.warmup:
+            e2e_ms.append(a.elapsed_time(b))
+    e2e = _max_over_ranks(torch, float(np.mean(e2e_ms)), ws)
+    h2d = (len(eps_axis) + len(a_axis)) * 8
+    d2h = int(out.size) * out.itemsize
+
+    flops_ps = fp32.flops_per_point_step()
+    total_units = points * ksteps * ws
+    value = total_units / (ms32 / 1e3)
+    line = None
+    if rank == 0:
+        achieved = points * ksteps * flops_ps / (float(np.mean(t32)) / 1e3) / 1e12
+        traffic = _traffic_from_profiles().get("fp32_dram_bytes_per_launch")
+        lat = sorted(t32)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms32, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"four-level Lindblad interferogram, {side}x{side} (eps, A) grid per GPU, "
+                                   f"RK4 {ksteps} steps on [0, {DURATION * nsteps / NSTEPS:g}], mean <|3><3|>",
+                       "points_per_gpu": points, "rk4_steps": ksteps, "parallelism": f"sweep shards x{ws}",
+                       "l2": "flushed (256 MiB write) between timed launches",
+                       "form": "FP32 state/RHS, FP64 time + drive phase + compensated average"},
+            "plain_fp64": {"value": total_units / (ms64 / 1e3), "ms_per_step": ms64},
+            "speedup_vs_plain_fp64": ms64 / ms32,
+            "max_abs_err_vs_fp64": err,
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peaks.get("fp32"), "unit": "TFLOP/s",
+                         "frac": achieved / peaks["fp32"] if peaks.get("fp32") else None,
+                         "traffic": traffic, "peak_source": "measured FFMA probe (gqis_probe_fma) in this run",
+                         "flops_per_point_step": flops_ps},
+            "peaks_measured_tflops": peaks,
+            "clocks": clocks,
+            "e2e": {"value": total_units / (e2e / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e},
+            "gpu_launches": args.steps,
+        }
+        if ws == 1 and not args.no_cpu_baseline:
+            ref = cpu_reference(steps=1, sample="c2_fp64_mean_sub128")
+            line["cpu_baseline"] = {"value": ref["points"] * ref["steps"] / ref["times"][0], "unit": UNIT,
+                                    "cores": ref["cores"], "kind": ref["kind"], "sample": ref["sample"]}
+        if ws == 1 and args.reference_gpu:
+            line["reference_kernel_gpu"] = reference_gpu_kernels()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line))
+    return 0
+
+
+def reference_gpu_kernels():
+    """The reference's own generated kernels for this workload, compiled for sm_100a, same GPU."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import ref_kernels
+    out = {}
+    for form, case in (("fp64", "c2_fp64_mean_full"), ("fp32", "c2_fp32_mean_full")):
+        if not ref_kernels.available(case, "gpu"):
+            out[form] = None
+            continue
+        ref_kernels.run_case(case, "gpu")
+        _, dt = ref_kernels.run_case(case, "gpu", repeats=2)
+        out[form] = {"ms_per_sweep": dt * 1e3, "value": SIDE * SIDE * NSTEPS / dt}
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
+    ap.add_argument("--side", type=int, default=SIDE)
+    ap.add_argument("--nsteps", type=int, default=NSTEPS)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--reference-gpu", action="store_true",
+                    help="also time the reference's generated kernels on this GPU")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,141 @@
+// gqis_module.cuh - the C-ABI entry points of one model module (include/gqis_b200.h).
+//
+// The generated translation unit defines, before including this file:
+//   GQ_MODEL        the emitted model struct
+//   GQ_FORM         FormFP64 or FormFP32
+//   GQ_SOLVER       an integrator type of gqis_fixed.cuh / gqis_adaptive.cuh
+//   GQ_SOLVER_ID    its GQIS_SOLVER_* number
+//   GQ_ADAPTIVE     1 for the persistent work-stealing adaptive kernels
+//   GQ_OUT, GQ_TRACE  output and trace mode
+//   GQ_MODEL_HASH   64-bit hash of the model text
+#pragma once
+
+#include <stdarg.h>
+#include <stdio.h>
+
+#include "gqis_fixed.cuh"
+#include "gqis_adaptive.cuh"
+
+namespace {
+
+thread_local char g_last_error[1024] = "";
+
+int fail(int code, const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_last_error, sizeof(g_last_error), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+    return fail(GQIS_ERR_CUDA, "%s: %s (%s)", what, cudaGetErrorString(e), cudaGetErrorName(e));
+}
+
+using Model = GQ_MODEL;
+using Form = GQ_FORM;
+
+#if GQ_ADAPTIVE
+constexpr auto kKernel = gqadaptive::sweep_adaptive_kernel<GQ_SOLVER, Model, Form, GQ_OUT, GQ_TRACE>;
+#else
+constexpr auto kKernel = gqfixed::sweep_fixed_kernel<GQ_SOLVER, Model, Form, GQ_OUT, GQ_TRACE>;
+#endif
+
+int check_desc(const gqis_sweep_desc* d) {
+    if (!d) return fail(GQIS_ERR_INVALID, "descriptor is NULL");
+    if (d->abi_version != GQIS_ABI_VERSION)
+        return fail(GQIS_ERR_INVALID, "descriptor ABI version %d, module expects %d", d->abi_version,
+                    GQIS_ABI_VERSION);
+    if (d->num_x < 1 || d->num_y < 1) return fail(GQIS_ERR_INVALID, "sweep axes must be non-empty");
+    const int64_t total = (int64_t)d->num_x * d->num_y;
+    if (d->point_begin < 0 || d->point_count < 0 || d->point_begin + d->point_count > total)
+        return fail(GQIS_ERR_INVALID, "point range [%lld, %lld) outside the %lld-point grid",
+                    (long long)d->point_begin, (long long)(d->point_begin + d->point_count),
+                    (long long)total);
+    if (d->num_steps < 1) return fail(GQIS_ERR_INVALID, "num_steps must be at least 1");
+    if (d->warmup_steps < 0 || d->warmup_steps > d->num_steps)
+        return fail(GQIS_ERR_INVALID, "warmup_steps must lie in [0, num_steps]");
+    if ((GQ_OUT == GQIS_OUT_MEAN || GQ_OUT == GQIS_OUT_MEAN_STATE) && d->warmup_steps >= d->num_steps)
+        return fail(GQIS_ERR_INVALID, "a mean output needs at least one step after warmup");
+    if (!(d->dt > 0.0) || !(d->dt < 1e300)) return fail(GQIS_ERR_INVALID, "dt must be positive and finite");
+    if (d->point_count == 0) return GQIS_OK;
+    if (!d->par_x || !d->par_y || !d->results) return fail(GQIS_ERR_INVALID, "par_x, par_y and results are required");
+    if (Model::kInitFromArray && !d->rho0) return fail(GQIS_ERR_INVALID, "this module reads rho0, which is NULL");
+    if (GQ_TRACE != GQIS_TRACE_NONE) {
+        if (!d->trace || d->num_trace < 0 || d->trace_stride < 1 || d->trace_offset < 0)
+            return fail(GQIS_ERR_INVALID, "trace buffer/stride/offset invalid");
+    }
+#if GQ_ADAPTIVE
+    if (!d->work_counter) return fail(GQIS_ERR_INVALID, "adaptive kernels need a zeroed work_counter");
+    if (!(d->solver_params[0] >= 0.0) || !(d->solver_params[1] >= 0.0) ||
+        !(d->solver_params[0] + d->solver_params[1] > 0.0) || !(d->solver_params[2] >= 1.0))
+        return fail(GQIS_ERR_INVALID, "adaptive parameters rtol/atol/max_substeps invalid");
+#endif
+    return GQIS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+__attribute__((visibility("default"))) const char* gqis_last_error(void) { return g_last_error; }
+
+__attribute__((visibility("default"))) int gqis_model_info_get(gqis_model_info* out) {
+    if (!out) return fail(GQIS_ERR_INVALID, "info pointer is NULL");
+    out->abi_version = GQIS_ABI_VERSION;
+    out->state_size = Model::S;
+    out->num_consts = Model::NCONST;
+    out->form = Form::id;
+    out->solver = GQ_SOLVER_ID;
+    out->output_mode = GQ_OUT;
+    out->trace_mode = GQ_TRACE;
+    out->init_from_array = Model::kInitFromArray ? 1 : 0;
+    out->block_threads = GQ_BLOCK;
+    out->model_hash = (uint64_t)GQ_MODEL_HASH;
+    out->registers_per_thread = 0;
+    out->sm_count = 0;
+    out->ctas_per_sm = 0;
+    cudaFuncAttributes attr;
+    cudaError_t e = cudaFuncGetAttributes(&attr, kKernel);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncGetAttributes");
+    out->registers_per_thread = attr.numRegs;
+    int dev = 0, sms = 0, ctas = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+        return cuda_fail(e, "cudaDeviceGetAttribute");
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas, kKernel, GQ_BLOCK, 0)) != cudaSuccess)
+        return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    out->sm_count = sms;
+    out->ctas_per_sm = ctas;
+    return GQIS_OK;
+}
+
+__attribute__((visibility("default"))) int gqis_sweep_launch(const gqis_sweep_desc* d, void* stream) {
+    int rc = check_desc(d);
+    if (rc != GQIS_OK || d->point_count == 0) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+#if GQ_ADAPTIVE
+    // Persistent grid: every resident CTA slot of the device, lanes refill themselves.
+    int dev = 0, sms = 0, ctas = 0;
+    cudaError_t e;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+        return cuda_fail(e, "cudaDeviceGetAttribute");
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas, kKernel, GQ_BLOCK, 0)) != cudaSuccess)
+        return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    if (ctas < 1) ctas = 1;
+    const int64_t needed = (d->point_count + GQ_BLOCK - 1) / GQ_BLOCK;
+    int64_t grid = (int64_t)sms * ctas;
+    if (grid > needed) grid = needed;
+    kKernel<<<(unsigned)grid, GQ_BLOCK, 0, st>>>(*d);
+#else
+    const int64_t grid = (d->point_count + GQ_BLOCK - 1) / GQ_BLOCK;
+    if (grid > 0x7fffffffLL) return fail(GQIS_ERR_TOO_LARGE, "too many points for one launch");
+    kKernel<<<(unsigned)grid, GQ_BLOCK, 0, st>>>(*d);
+#endif
+    cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) return cuda_fail(err, "sweep kernel launch");
+    return GQIS_OK;
+}
+
+}  // extern "C"

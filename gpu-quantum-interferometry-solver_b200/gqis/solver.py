@@ -1,0 +1,1077 @@
+"""``mesolve_2D`` and the shared sweep engine (drop-in for ``gqis/solver.py`` of GQIS).
+
+Call path of one sweep (reference ``gqis/solver.py:1712-2391``):
+
+1. validate the call (uniform ``tlist`` from zero, warmup, trace stride/offset);
+2. prepare and optimise the RHS (``rhs.compile_rhs``, cached);
+3. emit the model struct (``emit.emit_model``) and build the model module for the chosen
+   integrator, precision form, output and trace mode (``engine``, cached in memory and on disk);
+4. upload sweep axes, constants and initial states into torch CUDA tensors, launch through the
+   C ABI on the current torch stream, time the launch with CUDA events;
+5. check the outputs for non-finite values and return NumPy arrays (or CUDA tensors with
+   ``return_device=True``).
+
+``calibrate_timesteps`` wraps the call in the step-size search of ``gqis/solver.py:928-1341``.
+The precision form is chosen by ``precision`` (``"fp64"`` or ``"fp32"``); by default it follows
+``fp64``. The FP32 form keeps time, drive phase and the running averages in FP64.
+"""
+
+from __future__ import annotations
+
+import os
+import sys
+import time
+import warnings
+from dataclasses import dataclass, field
+
+import numpy as np
+import sympy as sp
+
+from ._options import OPTION_GROUPS, apply_option_groups
+from .cuda_solvers import TSIT5A_DEFAULTS, counts_steps, get_solver_spec, normalize_solver_name
+from .lindblad import build_independent_rho, build_reduced_lindblad_rhs, rho_matrix_to_independent_exprs
+from .rhs import _RHS_CODE_CACHE, CompiledRHS, compile_rhs as _compile_rhs_impl, runtime_const_values
+from . import emit
+
+__all__ = ["mesolve_2D", "compile_lindblad_rhs", "CompiledRHS", "build_independent_rho",
+           "build_reduced_lindblad_rhs", "rho_matrix_to_independent_exprs"]
+
+_KERNEL_CACHE: dict = {}
+_TIMESTEP_CALIBRATION_CACHE: dict = {}
+
+TIMESTEP_CALIBRATION_DEFAULTS = {
+    "rms_atol": 1e-3, "rms_rtol": 0.0,
+    "max_atol": 1e-2, "max_rtol": 0.0,
+    "sample_stride": 8,
+    "max_steps": 2**20,
+    "min_step_tol": 1e-12,
+    "bisection_steps": 2,
+    "full_grid_bisection": False,
+    "recalibrate_every": None,
+    "reset": False,
+    "on_fail": "warning",
+    "range_warning": True,
+}
+_CALIBRATION_MAX_HALVINGS = 6
+TIMESTEP_CALIBRATION_ODE_DEFAULTS = {"rms_atol": 1e-4, "max_atol": 1e-3}
+
+PRECISIONS = ("fp64", "fp32")
+
+
+def _compile_rhs(*args, **kwargs):
+    """Indirection so tests can count symbolic preparations."""
+    return _compile_rhs_impl(*args, **kwargs)
+
+
+def compile_lindblad_rhs(H, Drive, Col_Ops, mean_operator, sweep_symbols, *, const_values=None,
+                         runtime_consts=None, keep_symbolic_consts=None, auto_runtime_consts=False,
+                         rho0=None, pre_expand=True, collect_rho=False, factor_terms=False,
+                         cse_batch_size=None, cse_simplify=False, hoist_rho_independent=True,
+                         RHSreuse=True, symbolic_workers="auto", max_symbolic_workers=None):
+    """Prepare and optimise a Lindblad RHS without device code (``gqis/solver.py:1592-1627``).
+
+    ``mesolve_2D(compiled, tlist=..., var_arrays=...)`` then starts from code emission.
+    """
+    sweep_symbols = tuple(sweep_symbols)
+    if not 1 <= len(sweep_symbols) <= 2:
+        raise ValueError("sweep_symbols must contain one or two symbols.")
+    compiled, _ = _compile_rhs(
+        H, Drive, Col_Ops, mean_operator, sweep_symbols=sweep_symbols, const_values=const_values,
+        runtime_consts=runtime_consts, keep_symbolic_consts=keep_symbolic_consts,
+        auto_runtime_consts=auto_runtime_consts, rho0=rho0, pre_expand=pre_expand,
+        collect_rho=collect_rho, factor_terms=factor_terms, cse_batch_size=cse_batch_size,
+        cse_simplify=cse_simplify, hoist_rho_independent=hoist_rho_independent, reuse=RHSreuse,
+        symbolic_workers=symbolic_workers, max_symbolic_workers=max_symbolic_workers)
+    return compiled
+
+
+# ----------------------------------------------------------------------------------------
+# device seam
+# ----------------------------------------------------------------------------------------
+
+@dataclass
+class SweepLaunch:
+    """Everything one kernel launch needs; ``_device_run`` is the only code touching the GPU."""
+
+    entry: dict                 # kernel-cache entry: source text, loaded module
+    form: str
+    output_mode: str
+    trace_mode: object
+    state_size: int
+    par_x: object
+    par_y: object
+    consts: list
+    rho0: object
+    num_steps: int
+    warmup_steps: int
+    dt: float
+    t_in: float
+    trace_stride: int = 1
+    trace_offset: int = 0
+    num_trace: int = 0
+    solver_params: tuple = ()
+    adaptive: bool = False
+    count_steps: bool = False
+    return_device: bool = False
+    collect_timing: bool = False
+    extra: dict = field(default_factory=dict)
+
+
+def _load_kernel(entry):
+    """Build (nvcc, disk-cached) and load the module of a kernel-cache entry."""
+    if entry.get("module") is None:
+        from . import engine
+        entry["module"] = engine.load_module(entry["source"], extra_flags=entry.get("flags", ()))
+    return entry["module"]
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("The B200 sweep engine needs a CUDA device; none is visible "
+                           "(there is no CPU fallback).")
+    return torch
+
+
+def _as_device(torch, values, dtype, device):
+    if isinstance(values, torch.Tensor):
+        return values.to(device=device, dtype=dtype).contiguous()
+    return torch.as_tensor(np.ascontiguousarray(np.asarray(values)), dtype=dtype).to(device)
+
+
+def _device_buffers(launch: SweepLaunch, point_begin=0, point_count=None):
+    """Upload inputs and allocate outputs on the current device; returns ``(desc, tensors)``."""
+    from . import abi
+    torch = _torch()
+    device = torch.device("cuda", torch.cuda.current_device())
+    real = torch.float64 if launch.form == "fp64" else torch.float32
+    px = _as_device(torch, launch.par_x, torch.float64, device)
+    py = _as_device(torch, launch.par_y, torch.float64, device)
+    total = int(px.numel()) * int(py.numel())
+    npts = total - point_begin if point_count is None else int(point_count)
+    consts = (torch.tensor(launch.consts, dtype=torch.float64, device=device) if launch.consts else None)
+    rho0 = None
+    if launch.rho0 is not None:
+        rho0 = _as_device(torch, launch.rho0, real, device).reshape(total, launch.state_size)
+        rho0 = rho0[point_begin:point_begin + npts].contiguous()
+    width = 2 if launch.output_mode in ("mean", "final") else launch.state_size
+    results = torch.empty((npts, width), dtype=real, device=device)
+    trace = None
+    if launch.trace_mode is not None:
+        tw = 2 if launch.trace_mode == "observable" else launch.state_size
+        trace = torch.zeros((npts, launch.num_trace, tw), dtype=real, device=device)
+    counts = torch.zeros((npts, 2), dtype=torch.int32, device=device) if launch.count_steps else None
+    counter = torch.zeros(1, dtype=torch.int32, device=device) if launch.adaptive else None
+
+    desc = abi.SweepDesc()
+    desc.abi_version = abi.ABI_VERSION
+    desc.num_x, desc.num_y = int(px.numel()), int(py.numel())
+    desc.num_steps, desc.warmup_steps = int(launch.num_steps), int(launch.warmup_steps)
+    desc.trace_stride, desc.trace_offset = int(launch.trace_stride), int(launch.trace_offset)
+    desc.num_trace = int(launch.num_trace)
+    desc.point_begin, desc.point_count = int(point_begin), npts
+    desc.dt, desc.t_in = float(launch.dt), float(launch.t_in)
+    desc.par_x, desc.par_y = px.data_ptr(), py.data_ptr()
+    desc.consts = consts.data_ptr() if consts is not None else None
+    desc.rho0 = rho0.data_ptr() if rho0 is not None else None
+    desc.results = results.data_ptr()
+    desc.trace = trace.data_ptr() if trace is not None else None
+    desc.step_counts = counts.data_ptr() if counts is not None else None
+    desc.work_counter = counter.data_ptr() if counter is not None else None
+    for k, v in enumerate(launch.solver_params[:8]):
+        desc.solver_params[k] = float(v)
+    tensors = {"par_x": px, "par_y": py, "consts": consts, "rho0": rho0, "results": results,
+               "trace": trace, "step_counts": counts, "work_counter": counter}
+    return desc, tensors
+
+
+def _device_run(launch: SweepLaunch):
+    """Build/load the module, upload inputs, launch and return output tensors on the device.
+
+    Returns ``(results, trace, step_counts, gpu_seconds)``; ``results`` has shape (P, 2) or
+    (P, S), ``trace`` (P, num_trace, 2 or S), ``step_counts`` (P, 2) int32 or None.
+    """
+    torch = _torch()
+    module = _load_kernel(launch.entry)
+    desc, buf = _device_buffers(launch)
+    stream = torch.cuda.current_stream()
+    gpu_s = 0.0
+    if launch.collect_timing:
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+    module.launch(desc, stream.cuda_stream)
+    if launch.collect_timing:
+        stop.record(stream)
+        stop.synchronize()
+        gpu_s = start.elapsed_time(stop) / 1000.0
+    return buf["results"], buf["trace"], buf["step_counts"], gpu_s
+
+
+class PreparedSweep:
+    """A sweep set up once and launched many times on device-resident buffers.
+
+    ``prepare_sweep("mesolve_2D", *args, **kwargs)`` runs the front end and module build of the
+    call, uploads its inputs and allocates its outputs; ``launch()`` then only enqueues the kernel
+    on the current stream (used by bench.py, the serving loop and the parity tests).
+    ``point_begin`` / ``point_count`` restrict it to a slice of the flattened grid (sharding).
+    """
+
+    def __init__(self, launch: SweepLaunch, point_begin=0, point_count=None):
+        self.launch_spec = launch
+        self.module = _load_kernel(launch.entry)
+        self.desc, self.tensors = _device_buffers(launch, point_begin, point_count)
+        self.points = int(self.desc.point_count)
+        self.steps = int(launch.num_steps)
+        frag = launch.entry["frag"]
+        self.state_size = frag["state_size"]
+        self.rhs_flops = emit.count_rhs_flops(frag)
+        self.drive_flops = emit.count_drive_flops(frag)
+        self.solver = launch.entry["spec"].name
+
+    @property
+    def results(self):
+        return self.tensors["results"]
+
+    def reset(self):
+        if self.tensors["work_counter"] is not None:
+            self.tensors["work_counter"].zero_()
+
+    def launch(self, stream=None):
+        import torch
+        self.reset()
+        st = stream if stream is not None else torch.cuda.current_stream()
+        self.module.launch(self.desc, st.cuda_stream)
+
+    def flops_per_point_step(self):
+        """Algorithmic flops per point and RK4 step: 4 RHS + stage updates + 2 drive sets + <O>."""
+        S = self.state_size
+        return 4 * self.rhs_flops + 13 * S + 2 * self.drive_flops + 4
+
+
+def prepare_sweep(api, *args, point_begin=0, point_count=None, **kwargs):
+    """Set up a sweep for repeated device-resident launches (see :class:`PreparedSweep`)."""
+    holder = {}
+    kwargs["_prepare_only"] = holder
+    if api in ("odesolve_2D", "odesolve"):
+        from .gqis_ode_api import odesolve_2D
+        odesolve_2D(*args, **kwargs)
+    else:
+        mesolve_2D(*args, **kwargs)
+    return PreparedSweep(holder["launch"], point_begin, point_count)
+
+
+def _to_output(tensor, return_device):
+    if tensor is None:
+        return None
+    return tensor if return_device else tensor.cpu().numpy()
+
+
+def _all_finite(x):
+    if hasattr(x, "isfinite") and not isinstance(x, np.ndarray):
+        import torch
+        return bool(torch.isfinite(x).all())
+    return bool(np.all(np.isfinite(x)))
+
+
+def _beep():
+    print("\a", end="", flush=True)
+
+
+def _save_kernel(path_or_flag, source):
+    if not path_or_flag:
+        return None
+    if isinstance(path_or_flag, str) and path_or_flag.strip():
+        path = os.path.abspath(path_or_flag)
+    else:
+        main = getattr(sys.modules.get("__main__"), "__file__", None)
+        path = (os.path.join(os.path.dirname(os.path.abspath(main)),
+                             os.path.splitext(os.path.basename(main))[0] + "_Kernel.cu")
+                if main else os.path.abspath("Generated_Kernel.cu"))
+    with open(path, "w", encoding="utf-8", newline="\n") as f:
+        f.write(source)
+    return path
+
+
+def _print_timings(api_name, info, mode):
+    ode = {"miss": "new ODE", "hit": "reused ODE", "provided": "compiled ODE"}[info["cached_rhs"]]
+    kernel = "new kernel" if info["cached_kernel"] == "miss" else "reused kernel"
+    prep, gpu, total = info["rhs_stage_s"], info["gpu_kernel_s"], info["total_s"]
+
+    def show(s):
+        return f"{s * 1e3:.1f} ms" if s < 1.0 else f"{s:.2f} s"
+
+    if mode != "full":
+        print(f"{api_name}: preparation {show(prep)} ({ode}, {kernel}), GPU {show(gpu)}, total {show(total)}")
+        return
+    stages = [("symbolic ODE", info["ode_prepare_s"]), ("optimization", info["ode_optimize_s"]),
+              ("CUDA code", info["code_emit_s"]), ("kernel build", info["kernel_build_s"])]
+    stages.append(("setup", max(0.0, prep - sum(s for _, s in stages))))
+    print(f"{api_name} timings ({info['solver']}, {info['precision']}):")
+    print(f"  {'preparation':<16}{show(prep):>10}   {ode}, {kernel}")
+    for name, s in stages:
+        print(f"    {name:<14}{show(s):>10}")
+    print(f"  {'GPU calculation':<16}{show(gpu):>10}")
+    print(f"  {'other':<16}{show(max(0.0, total - prep - gpu)):>10}   transfer and checks")
+    print(f"  {'total':<16}{show(total):>10}")
+
+
+# ----------------------------------------------------------------------------------------
+# public entry point
+# ----------------------------------------------------------------------------------------
+
+def prebuild(api, *args, source_only=False, **kwargs):
+    """Compile the model module a ``mesolve_2D`` / ``odesolve_2D`` call would use, without a GPU.
+
+    Returns the path of the cached shared library, so a later process (or the same tree on
+    another machine) loads it without running nvcc; ``source_only=True`` returns
+    ``(source, nvcc_flags)`` instead, for parallel builds.
+    """
+    mode = "source" if source_only else True
+    kwargs.pop("calibrate_timesteps", None)
+    if api in ("odesolve_2D", "odesolve"):
+        from .gqis_ode_api import odesolve_2D
+        return odesolve_2D(*args, _prebuild_only=mode, **kwargs)
+    return mesolve_2D(*args, _prebuild_only=mode, **kwargs)
+
+
+def mesolve_2D(H, Drive=None, Col_Ops=None, mean_operator=None, tlist=None,
+               var_arrays=None, const_values=None, kernel_template_file=None, *,
+               RHSreuse=True, runtime_consts=None, keep_symbolic_consts=None,
+               auto_runtime_consts=False, output_mode="mean", solver="rk4",
+               solver_frequency=None, adaptive_options=None, unroll=False, fp64=False,
+               precision=None, pre_expand=True, collect_rho=False, factor_terms=False,
+               cse_batch_size=None, cse_simplify=False, hoist_rho_independent=True,
+               symbolic_workers="auto", max_symbolic_workers=None,
+               nvrtc_options=(), timings=False, return_timing_info=False, warmup_time=0.0,
+               rho0=None, rho0_var_arrays=None, rho0_values=None,
+               return_time_trace=False, time_trace_every=None,
+               time_trace_samples_per_period=None, solver_samples_per_period=None,
+               Actual_Kernel_Save=False, beep_on_error=False, ignore_non_finite_output=False,
+               t_in=0.0, return_device=False, calibrate_timesteps=None, consts=None, initial=None,
+               output=None, solver_options=None, codegen=None, diagnostics=None, _prebuild_only=False,
+               _prepare_only=None):
+    args = dict(locals())
+    groups = {name: args.pop(name) for name in OPTION_GROUPS}
+    args, _ = apply_option_groups(mesolve_2D, args, groups)
+    if args["output_mode"] not in {"mean", "final", "final_rho"}:
+        raise ValueError("output_mode must be 'mean', 'final', or 'final_rho'.")
+    if isinstance(H, CompiledRHS):
+        if H.kind != "lindblad":
+            raise ValueError("This CompiledRHS comes from compile_ode_rhs; pass it to odesolve_2D.")
+        args.update(H=None, compiled_rhs=H)
+    return _solve_symbolic_system(**args)
+
+
+def _resolve_precision(precision, fp64):
+    if precision is None:
+        return "fp64" if fp64 else "fp32"
+    p = str(precision).lower()
+    if p not in PRECISIONS:
+        raise ValueError(f"precision must be one of {PRECISIONS} or None.")
+    return p
+
+
+def _solve_symbolic_system(H, Drive, Col_Ops, mean_operator, tlist,
+                           var_arrays=None, const_values=None, kernel_template_file=None, *,
+                           RHSreuse=True, runtime_consts=None, keep_symbolic_consts=None,
+                           auto_runtime_consts=False, output_mode="mean", solver="rk4",
+                           solver_frequency=None, adaptive_options=None, unroll=False,
+                           fp64=False, precision=None,
+                           pre_expand=True, collect_rho=False, factor_terms=False,
+                           cse_batch_size=None, cse_simplify=False, hoist_rho_independent=True,
+                           symbolic_workers="auto", max_symbolic_workers=None,
+                           nvrtc_options=(), timings=False, return_timing_info=False, warmup_time=0.0,
+                           rho0=None, rho0_var_arrays=None, rho0_values=None,
+                           return_time_trace=False, time_trace_every=None,
+                           time_trace_samples_per_period=None, solver_samples_per_period=None,
+                           Actual_Kernel_Save=False, beep_on_error=False, ignore_non_finite_output=False,
+                           t_in=0.0, return_device=False, calibrate_timesteps=None, compiled_rhs=None,
+                           _ode_size=None, _state_trace=False, _time_trace_offset=0, _prebuild_only=False,
+                           _prepare_only=None):
+    """Solve a Lindblad master equation (or, through ``odesolve_2D``, a real ODE) on a 1-D or 2-D
+    parameter sweep, one independent time integration per point on the GPU.
+
+    Arguments, defaults and return shapes are those of the reference ``mesolve_2D``
+    (``gqis/solver.py:1739-1900``):
+
+    * result ``(num_X, num_Y)`` complex for ``"mean"`` / ``"final"``; ``(num_X, num_Y, N*N-1)``
+      real for ``"final_rho"`` (and ``"mean_state"`` from ``odesolve_2D``);
+    * with ``return_time_trace`` the tuple ``(result, trace, trace_t)``; with
+      ``return_timing_info`` the timing dict is appended;
+    * ``return_device=True`` returns torch CUDA tensors instead of NumPy arrays.
+
+    Additions of this engine: ``precision`` (``"fp64"`` or ``"fp32"``; default from ``fp64``),
+    the adaptive ``"dop853a"`` solver, and ``kernel_template_file``, which here names an extra
+    include directory (or a file in it) searched before the packaged CUDA templates.
+    """
+    if (calibrate_timesteps is not None and calibrate_timesteps is not False and not _prebuild_only
+            and _prepare_only is None):
+        return _solve_with_timestep_calibration(dict(locals()))
+    valid_modes = {"mean", "final", "final_rho", "mean_state"}
+    if output_mode not in valid_modes:
+        raise ValueError(f"Unsupported output_mode '{output_mode}'. Use one of: {sorted(valid_modes)}")
+    if not isinstance(unroll, (bool, np.bool_)):
+        raise ValueError("unroll must be True or False.")
+    unroll = bool(unroll)
+    template_dir = None
+    if kernel_template_file is not None:
+        if not os.path.exists(kernel_template_file):
+            raise FileNotFoundError(f"CUDA kernel template was not found: {kernel_template_file}")
+        template_dir = (kernel_template_file if os.path.isdir(kernel_template_file)
+                        else os.path.dirname(os.path.abspath(kernel_template_file)))
+    form = _resolve_precision(precision, fp64)
+    t_in = float(t_in)
+    if not np.isfinite(t_in):
+        raise ValueError("t_in must be finite.")
+
+    var_arrays = {} if var_arrays is None else dict(var_arrays)
+    for sym, arr in (rho0_var_arrays or {}).items():
+        if sym in var_arrays:
+            raise ValueError(f"Symbol {sym} is present in both var_arrays and rho0_var_arrays.")
+        var_arrays[sym] = arr
+    const_values = {} if const_values is None else const_values
+    if rho0 is not None and rho0_values is not None:
+        raise ValueError("Use either rho0 or rho0_values, not both.")
+    uses_rho0_values = rho0_values is not None
+    if not var_arrays:
+        raise ValueError("var_arrays or rho0_var_arrays must contain at least one sweep array (ParX).")
+    if len(var_arrays) > 2:
+        raise ValueError("Only 2 total sweep arrays are supported across var_arrays and rho0_var_arrays.")
+    if compiled_rhs is None:
+        if H is None or Drive is None or Col_Ops is None or mean_operator is None:
+            raise TypeError("Give H, Drive, Col_Ops and mean_operator, or a CompiledRHS.")
+    else:
+        if any(x is not None for x in (H, Drive, Col_Ops, mean_operator)):
+            raise ValueError("With a CompiledRHS, do not pass the model (H, Drive, Col_Ops, "
+                             "mean_operator) again.")
+        if const_values or keep_symbolic_consts is not None or auto_runtime_consts or rho0 is not None:
+            raise ValueError("const_values, keep_symbolic_consts, auto_runtime_consts and rho0 are "
+                             "fixed when the RHS is compiled; give values of constants kept "
+                             "symbolic through runtime_consts.")
+        if tuple(var_arrays) != compiled_rhs.sweep_symbols:
+            raise ValueError(f"The sweep arrays must be for {compiled_rhs.sweep_symbols}, in the "
+                             "order given when the RHS was compiled.")
+
+    # ---- time grid (gqis/solver.py:1951-2010)
+    if tlist is None:
+        raise ValueError("tlist is required for fixed-step integration.")
+    n_t = int(len(tlist))
+    if n_t < 2:
+        raise ValueError("tlist must contain at least two time samples.")
+    t_raw = np.asarray(tlist.cpu() if hasattr(tlist, "cpu") else tlist)
+    t_host = np.asarray(t_raw, dtype=np.float64)
+    if t_host.ndim != 1 or not np.all(np.isfinite(t_host)):
+        raise ValueError("tlist must be a finite one-dimensional array.")
+    diffs = np.diff(t_host)
+    if np.any(diffs <= 0.0):
+        raise ValueError("tlist must be strictly increasing.")
+    in_dtype = t_raw.dtype if np.issubdtype(t_raw.dtype, np.floating) else np.dtype(np.float64)
+    tol = 8.0 * np.finfo(in_dtype).eps * max(1.0, float(np.max(np.abs(t_host))))
+    dt_host = float((t_host[-1] - t_host[0]) / (n_t - 1))
+    spec = get_solver_spec(solver, frequency=solver_frequency, step_size=dt_host,
+                           adaptive_options=adaptive_options, fp64=form == "fp64")
+    if not np.isclose(t_host[0], 0.0, rtol=0.0, atol=tol):
+        raise ValueError("tlist must begin at zero; the CUDA kernel derives stage times from the step index.")
+    if not np.allclose(diffs, dt_host, rtol=1.0e-6, atol=tol):
+        raise ValueError("tlist must be uniformly spaced because the GPU solver uses one fixed dt.")
+    num_steps = n_t - 1
+    warmup_time = float(warmup_time)
+    if warmup_time < 0.0 or warmup_time > 1.0:
+        raise ValueError("warmup_time must be within [0, 1].")
+    warmup_steps = num_steps if warmup_time >= 1.0 else int(np.floor(warmup_time * num_steps))
+    warmup_steps = max(0, min(num_steps, warmup_steps))
+    return_time_trace = bool(return_time_trace)
+    if time_trace_every is not None and time_trace_samples_per_period is not None:
+        raise ValueError("Use either time_trace_every or time_trace_samples_per_period, not both.")
+    if time_trace_samples_per_period is not None:
+        if solver_samples_per_period is None:
+            raise ValueError("solver_samples_per_period is required when "
+                             "time_trace_samples_per_period is used.")
+        sspp, tspp = int(solver_samples_per_period), int(time_trace_samples_per_period)
+        if sspp <= 0 or tspp <= 0:
+            raise ValueError("solver_samples_per_period and time_trace_samples_per_period must be positive.")
+        stride = max(1, int(round(sspp / tspp)))
+    elif time_trace_every is not None:
+        stride = int(time_trace_every)
+        if stride <= 0:
+            raise ValueError("time_trace_every must be a positive integer.")
+    else:
+        stride = 1
+    offset = int(_time_trace_offset)
+    num_trace = int(np.ceil((num_steps - offset) / stride)) if return_time_trace else 0
+
+    mode = output_mode
+    if output_mode == "mean" and warmup_steps >= num_steps:
+        mode = "final"
+    if output_mode == "mean_state" and warmup_steps >= num_steps:
+        mode = "final_rho"
+
+    if timings not in (False, None, True, "compact", "full"):
+        raise ValueError("timings must be False, True, 'compact' or 'full'.")
+    collect = bool(timings or return_timing_info)
+    t_total = time.time()
+
+    # ---- 1) symbolic preparation
+    if compiled_rhs is None:
+        compiled, rhs_status = _compile_rhs(
+            H, Drive, Col_Ops, mean_operator, sweep_symbols=tuple(var_arrays), const_values=const_values,
+            runtime_consts=runtime_consts, keep_symbolic_consts=keep_symbolic_consts,
+            auto_runtime_consts=auto_runtime_consts, rho0=rho0, ode_size=_ode_size,
+            pre_expand=pre_expand, collect_rho=collect_rho, factor_terms=factor_terms,
+            cse_batch_size=cse_batch_size, cse_simplify=cse_simplify,
+            hoist_rho_independent=hoist_rho_independent, reuse=RHSreuse,
+            symbolic_workers=symbolic_workers, max_symbolic_workers=max_symbolic_workers)
+    else:
+        compiled, rhs_status = compiled_rhs, "provided"
+    stages = (dict(compiled.timings) if rhs_status == "miss" else {"ode_prepare_s": 0.0, "ode_optimize_s": 0.0})
+    const_vals = runtime_const_values(compiled, runtime_consts, const_values,
+                                      use_defaults=compiled_rhs is not None)
+
+    # ---- 2) model emission
+    t0 = time.time()
+    ekey = ("b200", bool(uses_rho0_values))
+    if RHSreuse and ekey in compiled.emitted:
+        frag, stages["emit_s"] = compiled.emitted[ekey], 0.0
+    else:
+        frag = emit.emit_model(compiled, uses_rho0_values)
+        if RHSreuse:
+            compiled.emitted[ekey] = frag
+        stages["emit_s"] = time.time() - t0
+    codegen_s = stages["ode_prepare_s"] + stages["ode_optimize_s"] + stages["emit_s"]
+
+    # ---- 3) module (kernel) for this variant
+    trace_mode = ("state" if _state_trace else "observable") if return_time_trace else None
+    count = spec.adaptive and counts_steps(adaptive_options)
+    flags = tuple([nvrtc_options] if isinstance(nvrtc_options, str) else nvrtc_options)
+    if template_dir:
+        flags = (f"-I{template_dir}",) + flags
+    tmtime = os.path.getmtime(kernel_template_file) if kernel_template_file else None
+    kkey = ("b200_kernel_v1", compiled.cache_key, bool(uses_rho0_values), mode, spec.name, unroll,
+            form, trace_mode, flags, tmtime)
+    kernel_status = "miss"
+    t_build = time.time()
+    entry = _KERNEL_CACHE.get(kkey) if RHSreuse else None
+    if entry is None:
+        from . import engine
+        entry = {"source": engine.module_source(frag, spec, form, mode, trace_mode, unroll),
+                 "module": None, "flags": flags + (("-DGQ_FULL_UNROLL=1",) if unroll else ()),
+                 "frag": frag, "spec": spec}
+        if RHSreuse:
+            _KERNEL_CACHE[kkey] = entry
+    else:
+        kernel_status = "hit"
+    saved = _save_kernel(Actual_Kernel_Save, entry["source"])
+    if _prebuild_only:  # build the module for later processes; no device is touched
+        if _prebuild_only == "source":
+            return entry["source"], entry["flags"]
+        from . import engine
+        return engine.build_module(entry["source"], extra_flags=entry["flags"])
+
+    # ---- 4) inputs and launch
+    axes = list(var_arrays.values())
+
+    def host_axis(a):
+        return a if hasattr(a, "data_ptr") else np.asarray(a, dtype=np.float64).reshape(-1)
+
+    par_x = host_axis(axes[0])
+    par_y = host_axis(axes[1]) if len(axes) > 1 else np.zeros(1)
+    nx, ny = int(len(par_x)), int(len(par_y))
+    rho0_arr = None
+    if uses_rho0_values:
+        shape = tuple(rho0_values.shape) if hasattr(rho0_values, "shape") else np.shape(rho0_values)
+        S = compiled.state_size
+        if not (shape == (nx, ny, S) or (shape == (nx, S) and ny == 1)):
+            raise ValueError(f"rho0_values must have shape ({nx}, {ny}, {S}) or ({nx}, {S}) "
+                             f"when num_Y=1; got {tuple(shape)}.")
+        rho0_arr = rho0_values if hasattr(rho0_values, "data_ptr") else np.asarray(rho0_values, dtype=np.float64)
+    used = frag["used_const_indices"]
+    consts_eff = [const_vals[i] for i in used] if used else []
+    if spec.adaptive:
+        params = tuple(spec.parameters)
+    elif spec.parameters:
+        params = tuple(spec.parameters)
+    else:
+        params = ()
+    launch = SweepLaunch(entry=entry, form=form, output_mode=mode, trace_mode=trace_mode,
+                         state_size=compiled.state_size, par_x=par_x, par_y=par_y, consts=consts_eff,
+                         rho0=rho0_arr, num_steps=num_steps, warmup_steps=warmup_steps, dt=dt_host,
+                         t_in=t_in, trace_stride=stride, trace_offset=offset, num_trace=num_trace,
+                         solver_params=params, adaptive=spec.adaptive, count_steps=count,
+                         return_device=bool(return_device), collect_timing=collect)
+    if _prepare_only is not None:
+        _prepare_only["launch"] = launch
+        return None
+    _load_kernel(entry)
+    stage_build = time.time() - t_build
+    rhs_stage_s = time.time() - t_total
+    results, trace, counts, gpu_s = _device_run(launch)
+
+    # ---- 5) outputs
+    cplx = mode in ("mean", "final")
+    S = compiled.state_size
+
+    def shape_result(x):
+        if x is None:
+            return None
+        if hasattr(x, "reshape") and not isinstance(x, np.ndarray):
+            import torch
+            if cplx:
+                return torch.view_as_complex(x.reshape(nx, ny, 2).contiguous())
+            return x.reshape(nx, ny, S)
+        x = np.asarray(x)
+        if cplx:
+            x = x.reshape(nx, ny, 2)
+            return x[..., 0] + 1j * x[..., 1]
+        return x.reshape(nx, ny, S)
+
+    def shape_trace(x):
+        if x is None:
+            return None
+        if hasattr(x, "reshape") and not isinstance(x, np.ndarray):
+            import torch
+            if trace_mode == "observable":
+                return torch.view_as_complex(x.reshape(nx, ny, num_trace, 2).contiguous())
+            return x.reshape(nx, ny, num_trace, S)
+        x = np.asarray(x)
+        if trace_mode == "observable":
+            x = x.reshape(nx, ny, num_trace, 2)
+            return x[..., 0] + 1j * x[..., 1]
+        return x.reshape(nx, ny, num_trace, S)
+
+    res = shape_result(results)
+    tr = shape_trace(trace) if return_time_trace else None
+    if not return_device:
+        res = _to_output(res, False) if not isinstance(res, np.ndarray) else res
+        tr = _to_output(tr, False) if (tr is not None and not isinstance(tr, np.ndarray)) else tr
+    if cplx and isinstance(res, np.ndarray):
+        res = res.astype(np.complex128 if form == "fp64" else np.complex64, copy=False)
+        if tr is not None and trace_mode == "observable":
+            tr = tr.astype(np.complex128 if form == "fp64" else np.complex64, copy=False)
+    if not _all_finite(res) and not ignore_non_finite_output:
+        if beep_on_error:
+            _beep()
+        raise RuntimeError("Non-finite values detected in mesolve_2D output. Try reducing dt "
+                           "(increase time samples) or check model parameters/RHS.")
+    if return_time_trace and not _all_finite(tr) and not ignore_non_finite_output:
+        if beep_on_error:
+            _beep()
+        raise RuntimeError("Non-finite values detected in mesolve_2D time trace. Try reducing dt "
+                           "(increase time samples) or check model parameters/RHS.")
+
+    info = None
+    if collect:
+        info = {"rhs_stage_s": rhs_stage_s, "gpu_kernel_s": gpu_s, "rhs_codegen_s": codegen_s,
+                "total_s": time.time() - t_total, "ode_prepare_s": stages["ode_prepare_s"],
+                "ode_optimize_s": stages["ode_optimize_s"], "code_emit_s": stages["emit_s"],
+                "kernel_build_s": stage_build, "cached_rhs": rhs_status, "cached_kernel": kernel_status,
+                "solver": spec.name, "solver_frequency": solver_frequency, "unroll": unroll,
+                "precision": form, "rhs_flops": emit.count_rhs_flops(frag)}
+        module = entry.get("module")
+        if module is not None:
+            mi = module.info()
+            info.update(registers_per_thread=mi.registers_per_thread, ctas_per_sm=mi.ctas_per_sm,
+                        module_path=str(module.path))
+        if counts is not None:
+            c = counts if isinstance(counts, np.ndarray) else counts.cpu().numpy()
+            c = c.reshape(nx, ny, 2)
+            info["adaptive_steps"] = {"accepted": c[..., 0], "rejected": c[..., 1]}
+    if timings:
+        _print_timings("mesolve_2D" if _ode_size is None else "odesolve_2D", info, timings)
+    if saved:
+        print(f"Generated kernel saved to: {saved}")
+    if return_time_trace:
+        steps = np.arange(num_trace, dtype=np.float64 if form == "fp64" else np.float32) * stride
+        trace_t = t_in + (steps + 1.0 + offset) * dt_host
+        out = (res, tr, trace_t)
+        return (*out, info) if return_timing_info else out
+    if return_timing_info:
+        return res, info
+    return res
+
+
+
+
+# ----------------------------------------------------------------------------------------
+# calibrate_timesteps (gqis/solver.py:928-1341)
+# ----------------------------------------------------------------------------------------
+
+def _timestep_calibration_settings(value, ode=False):
+    """Validated ``calibrate_timesteps`` settings merged with the defaults."""
+    settings = dict(TIMESTEP_CALIBRATION_DEFAULTS)
+    if ode:
+        settings.update(TIMESTEP_CALIBRATION_ODE_DEFAULTS)
+    if value is not True:
+        if not isinstance(value, dict):
+            raise TypeError("calibrate_timesteps must be True, None or a dict of settings.")
+        unknown = set(value) - set(settings)
+        if unknown:
+            raise ValueError(f"Unknown calibrate_timesteps setting(s) {sorted(unknown)}. "
+                             f"Valid settings: {', '.join(settings)}.")
+        settings.update(value)
+    for name in ("rms_atol", "rms_rtol", "max_atol", "max_rtol"):
+        settings[name] = float(settings[name])
+        if settings[name] < 0.0:
+            raise ValueError(f"calibrate_timesteps {name} must be non-negative.")
+    settings["check_rms"] = settings["rms_atol"] > 0.0 or settings["rms_rtol"] > 0.0
+    settings["check_max"] = settings["max_atol"] > 0.0 or settings["max_rtol"] > 0.0
+    if not (settings["check_rms"] or settings["check_max"]):
+        raise ValueError("calibrate_timesteps needs at least one non-zero RMS or max tolerance.")
+    settings["sample_stride"] = int(settings["sample_stride"])
+    settings["max_steps"] = int(settings["max_steps"])
+    settings["min_step_tol"] = float(settings["min_step_tol"])
+    if settings["sample_stride"] < 1 or settings["max_steps"] < 1 or not settings["min_step_tol"] > 0.0:
+        raise ValueError("calibrate_timesteps sample_stride, max_steps and min_step_tol must be positive.")
+    settings["bisection_steps"] = int(settings["bisection_steps"])
+    if settings["bisection_steps"] < 0:
+        raise ValueError("calibrate_timesteps bisection_steps must be zero or a positive integer.")
+    settings["full_grid_bisection"] = bool(settings["full_grid_bisection"])
+    every = settings["recalibrate_every"]
+    if every is not None and int(every) < 1:
+        raise ValueError("calibrate_timesteps recalibrate_every must be None or a positive integer.")
+    settings["recalibrate_every"] = None if every is None else int(every)
+    if settings["on_fail"] not in {"warning", "ignore", "error"}:
+        raise ValueError("calibrate_timesteps on_fail must be 'warning', 'ignore' or 'error'.")
+    return settings
+
+
+def _is_adaptive(args):
+    return get_solver_spec(args["solver"]).adaptive
+
+
+def _timestep_calibration_key(args, settings):
+    """Model + accuracy request, independent of code-generation options."""
+    def key(e):
+        if isinstance(e, dict):
+            return frozenset((k, sp.sympify(v)) for k, v in e.items())
+        if isinstance(e, (list, tuple)):
+            return tuple(sp.sympify(x) for x in e)
+        if isinstance(e, sp.MatrixBase):
+            return e.shape, tuple(e)
+        return sp.sympify(e)
+
+    cv = args["const_values"] or {}
+    keep = args["keep_symbolic_consts"]
+    kept = set(args["runtime_consts"] or {})
+    if args["auto_runtime_consts"] or keep in ("all", "auto", "const_values"):
+        kept |= set(cv)
+    elif keep is not None:
+        kept |= set(keep)
+    fixed = tuple(sorted((str(k), float(v)) for k, v in cv.items() if k not in kept))
+    sweeps = tuple(str(s) for s in (args["var_arrays"] or {})) + tuple(
+        str(s) for s in (args["rho0_var_arrays"] or {}))
+    if args.get("compiled_rhs") is not None:
+        model = (args["compiled_rhs"].cache_key,)
+    else:
+        model = (key(args["H"]), key(args["Drive"]), tuple(key(L) for L in args["Col_Ops"]),
+                 key(args["mean_operator"]), key(args["rho0"]) if args["rho0"] is not None else None, fixed)
+    spec = get_solver_spec(args["solver"])
+    adaptive = None
+    if spec.adaptive:
+        opts = {**TSIT5A_DEFAULTS, **(args["adaptive_options"] or {})}
+        rtol, atol = float(opts["step_rtol"]), float(opts["step_atol"])
+        adaptive = (atol / rtol if rtol > 0.0 else np.inf, int(opts["max_substeps"]), settings["min_step_tol"])
+    return ("b200_timestep_calibration_v1", *model, sweeps, spec.name, adaptive, bool(args["fp64"]),
+            args.get("precision"), args["output_mode"], float(args["warmup_time"]), args["_ode_size"],
+            *(settings[n] for n in ("rms_atol", "rms_rtol", "max_atol", "max_rtol", "sample_stride",
+                                   "max_steps", "bisection_steps", "full_grid_bisection")))
+
+
+def _step_tolerance(args):
+    opts = {**TSIT5A_DEFAULTS, **(args["adaptive_options"] or {})}
+    return max(float(opts["step_rtol"]), float(opts["step_atol"]))
+
+
+def _scaled_adaptive_options(args, tol):
+    """adaptive_options with step_rtol and step_atol scaled together so the larger equals tol."""
+    opts = dict(args["adaptive_options"] or {})
+    merged = {**TSIT5A_DEFAULTS, **opts}
+    scale = tol / _step_tolerance(args)
+    opts.update(step_rtol=float(merged["step_rtol"]) * scale, step_atol=float(merged["step_atol"]) * scale)
+    return opts
+
+
+def _sweep_ranges(args):
+    out = []
+    for name in ("var_arrays", "rho0_var_arrays"):
+        for v in (args[name] or {}).values():
+            v = v if hasattr(v, "min") else np.asarray(v)
+            out.append((float(v.min()), float(v.max())))
+    return tuple(out)
+
+
+def _undersampled_arguments(args, stride):
+    """Arguments restricted to every stride-th point of each sweep axis (axis ends kept)."""
+    test = dict(args)
+    test.update(calibrate_timesteps=None, return_time_trace=False, return_timing_info=False, timings=False,
+                return_device=False, ignore_non_finite_output=True, Actual_Kernel_Save=False,
+                beep_on_error=False)
+
+    def picks(n):
+        idx = list(range(0, n, stride))
+        return idx if idx[-1] == n - 1 else idx + [n - 1]
+
+    def take(values, idx):
+        return [values[i] for i in idx] if isinstance(values, (list, tuple)) else values[idx]
+
+    axes, full = [], True
+    for name in ("var_arrays", "rho0_var_arrays"):
+        if args[name]:
+            test[name] = {}
+            for sym, values in args[name].items():
+                axes.append(picks(len(values)))
+                full = full and len(axes[-1]) == len(values)
+                test[name][sym] = take(values, axes[-1])
+    if args["rho0_values"] is not None:
+        v = args["rho0_values"]
+        v = v if hasattr(v, "ndim") else np.asarray(v)
+        v = v[axes[0]] if axes else v
+        test["rho0_values"] = v[:, axes[1]] if v.ndim == 3 and len(axes) > 1 else v
+    return test, full
+
+
+def _calibrate_timestep(args, settings, base_steps, duration):
+    """Coarsest resolution whose undersampled map meets the limits (``gqis/solver.py:1066-1216``).
+
+    Fixed-step solvers refine the step count by 2 (Richardson estimate with the method order,
+    order 1 for mean outputs); adaptive solvers refine 1/tolerance by 10 (error ~ tolerance).
+    A passing bracket is narrowed by ``bisection_steps`` geometric bisections.
+    """
+    start = time.time()
+    test, full_grid = _undersampled_arguments(args, settings["sample_stride"])
+    adaptive = _is_adaptive(args)
+    if adaptive:
+        factor, order = 10.0, 1
+        base, x_limit, label = 1.0 / _step_tolerance(args), 1.0 / settings["min_step_tol"], "step_tol"
+    else:
+        mean = args.get("output_mode") in ("mean", "mean_state") and float(args.get("warmup_time", 0.0)) < 1.0
+        factor, order = 2, (1 if mean else get_solver_spec(args["solver"]).order)
+        base, x_limit, label = base_steps, settings["max_steps"], "steps"
+
+    def value(x):
+        return 1.0 / x if adaptive else x
+
+    def coarser(x):
+        return x / factor if adaptive else x // 2
+
+    stored = {}
+
+    def run(x):
+        if adaptive:
+            test["adaptive_options"] = _scaled_adaptive_options(args, value(x))
+        else:
+            test["tlist"] = np.linspace(0.0, duration, x + 1)
+        r = np.asarray(_solve_symbolic_system(**test))
+        if full_grid:
+            stored[value(x)] = r
+        return r
+
+    def check(x, coarse, fine_x, fine):
+        rec = {label: value(x), "rms": np.inf, "max": np.inf}
+        if not (np.all(np.isfinite(coarse)) and np.all(np.isfinite(fine))):
+            return rec, False
+        scale = 1.0 / (1.0 - (x / fine_x) ** order)
+        diff = np.abs(fine - coarse) * scale
+        mag = np.abs(fine)
+        rec.update(rms=float(np.sqrt(np.mean(diff**2))), max=float(np.max(diff)))
+        rms_lim = settings["rms_atol"] + settings["rms_rtol"] * float(np.sqrt(np.mean(mag**2)))
+        max_lim = settings["max_atol"] + settings["max_rtol"] * float(np.max(mag))
+        ok = ((not settings["check_rms"] or rec["rms"] <= rms_lim)
+              and (not settings["check_max"] or rec["max"] <= max_lim))
+        return rec, ok
+
+    x, coarse = base, run(base)
+    tested, status, accepted = [], None, None
+    ref_x = ref = None
+    while status is None:
+        if factor * x > x_limit:
+            status, accepted = ("min_step_tol" if adaptive else "max_steps"), x
+            break
+        fine = run(factor * x)
+        if adaptive and np.all(np.isfinite(coarse)) and not np.all(np.isfinite(fine)):
+            status, accepted = "max_substeps", x
+            break
+        rec, ok = check(x, coarse, factor * x, fine)
+        tested.append(rec)
+        if ok:
+            status, accepted = "converged", x
+            ref_x, ref = factor * x, fine
+        elif len(tested) > 1 and np.isfinite(rec["rms"]) and rec["rms"] >= tested[-2]["rms"]:
+            best = min(tested, key=lambda r: r["rms"])
+            status, accepted = "precision_floor", (1.0 / best[label] if adaptive else best[label])
+        x, coarse = factor * x, fine
+
+    doubling = accepted
+    if status == "converged" and settings["bisection_steps"] > 0 and (settings["full_grid_bisection"] or not full_grid):
+        def passes(cand):
+            rec, ok = check(cand, run(cand), ref_x, ref)
+            tested.append({**rec, f"reference_{label}": value(ref_x)})
+            return ok
+
+        failing = coarser(accepted) if accepted > base else None
+        halvings = 0
+        while failing is None and (adaptive or accepted >= 2) and halvings < _CALIBRATION_MAX_HALVINGS:
+            halvings += 1
+            cand = coarser(accepted)
+            if passes(cand):
+                accepted = cand
+            else:
+                failing = cand
+        for _ in range(settings["bisection_steps"] if failing is not None else 0):
+            cand = np.sqrt(failing * accepted)
+            cand = float(cand) if adaptive else int(round(cand))
+            if cand <= failing or cand >= accepted:
+                break
+            if passes(cand):
+                accepted = cand
+            else:
+                failing = cand
+
+    info = {"status": status, "tested": tested, "test_grid": coarse.shape[:2],
+            "calibration_s": time.time() - start, "full_grid_results": stored}
+    if adaptive:
+        info.update(step_tol=value(accepted), doubling_step_tol=value(doubling), start_step_tol=value(base))
+    else:
+        info.update(steps=accepted, dt=duration / accepted, doubling_steps=doubling)
+
+    def describe(x):
+        return f"step tolerance {value(x):.2e}" if adaptive else f"{x} steps"
+
+    if status != "converged":
+        def limit(kind):
+            atol, rtol = settings[f"{kind}_atol"], settings[f"{kind}_rtol"]
+            return f"{'RMS' if kind == 'rms' else 'max'} {atol:g}" + (f" + {rtol:g} relative" if rtol else "")
+        requested = ", ".join(limit(k) for k in ("rms", "max") if settings[f"check_{k}"])
+        reason = {"precision_floor": "does not converge",
+                  "max_steps": "is not reached within max_steps",
+                  "min_step_tol": "is not reached above min_step_tol",
+                  "max_substeps": ("needs more than max_substeps steps per output interval "
+                                   "(increase adaptive_options max_substeps)")}[status]
+        if tested:
+            best = next((r for r in tested if r[label] == value(accepted)), tested[-1])
+            achieved = (f"best achieved RMS {best['rms']:.2e}, max {best['max']:.2e} with {describe(accepted)}")
+        else:
+            achieved = f"no refinement beyond {describe(accepted)} was possible"
+        message = f"calibrate_timesteps: requested precision ({requested}) {reason}; {achieved}."
+        if status == "precision_floor" and not args["fp64"]:
+            message += " If better precision is required, consider switching to fp64=True."
+        if settings["on_fail"] == "error":
+            raise RuntimeError(message)
+        if settings["on_fail"] == "warning":
+            warnings.warn(message, RuntimeWarning, stacklevel=4)
+    return info
+
+
+def _solve_with_timestep_calibration(args):
+    """Pick a uniform step (or adaptive tolerance) on a subgrid, then run the full sweep."""
+    settings = _timestep_calibration_settings(args["calibrate_timesteps"], ode=args["_ode_size"] is not None)
+    tl = np.asarray(args["tlist"], dtype=np.float64)
+    if tl.ndim != 1 or len(tl) < 2:
+        raise ValueError("tlist must be a one-dimensional array with at least two samples.")
+    base_steps, duration = len(tl) - 1, float(tl[-1] - tl[0])
+    adaptive = _is_adaptive(args)
+    key = _timestep_calibration_key(args, settings)
+    entry = None if settings["reset"] else _TIMESTEP_CALIBRATION_CACHE.get(key)
+    calls = entry["calls"] if entry else 0
+    every = settings["recalibrate_every"]
+    ranges = _sweep_ranges(args)
+    info = None
+    if entry is None or (every is not None and calls % every == 0):
+        info = _calibrate_timestep(args, settings, base_steps, duration)
+        found = info["step_tol"] if adaptive else info["dt"]
+        stored = found if entry is None else min(entry["value"], found)
+        if entry is not None:
+            ranges = tuple((min(a[0], b[0]), max(a[1], b[1])) for a, b in zip(entry["ranges"], ranges))
+        entry = {"value": stored, "ranges": ranges, "range_warned": False}
+    else:
+        stored = entry["value"]
+        outside = any(lo < olo or hi > ohi for (lo, hi), (olo, ohi) in zip(ranges, entry["ranges"]))
+        if outside and settings["range_warning"] and not entry["range_warned"]:
+            entry["range_warned"] = True
+            warnings.warn("calibrate_timesteps: the sweep range extends beyond the range used for calibration; "
+                          "the stored step is reused without a new test. Use reset=True or recalibrate_every "
+                          "to test the new range.", RuntimeWarning, stacklevel=3)
+    entry["calls"] = calls + 1
+    _TIMESTEP_CALIBRATION_CACHE[key] = entry
+
+    run_args = dict(args, calibrate_timesteps=None)
+    if adaptive:
+        aligned, chosen = False, stored
+
+        def configure(tol):
+            run_args["adaptive_options"] = _scaled_adaptive_options(args, tol)
+        start_text = f"step tolerance {info['start_step_tol']:.2e}" if info else ""
+        chosen_text = f"step tolerance {chosen:.2e}"
+    else:
+        aligned = bool(args["return_time_trace"])
+        chosen = int(np.ceil(duration / stored * (1.0 - 1e-9)))
+        if settings["bisection_steps"] == 0 or aligned:
+            chosen = max(base_steps, chosen)
+        fac = 1
+        if aligned:
+            while base_steps * fac < chosen and base_steps * fac < settings["max_steps"]:
+                fac *= 2
+            chosen = base_steps * fac
+        chosen = min(chosen, max(base_steps, settings["max_steps"]))
+        if aligned and fac > 1:
+            if args["time_trace_samples_per_period"] is not None:
+                stride = max(1, int(round(int(args["solver_samples_per_period"])
+                                          / int(args["time_trace_samples_per_period"]))))
+            else:
+                stride = int(args["time_trace_every"] or 1)
+            run_args.update(time_trace_every=stride * fac, time_trace_samples_per_period=None,
+                            solver_samples_per_period=None, _time_trace_offset=fac - 1)
+
+        def configure(steps):
+            run_args["tlist"] = np.linspace(0.0, duration, steps + 1)
+        start_text = f"{base_steps} steps"
+        chosen_text = f"{chosen} steps"
+    configure(chosen)
+    if info is not None and args["timings"]:
+        last = (f"; last RMS/max change {info['tested'][-1]['rms']:.2e}/{info['tested'][-1]['max']:.2e}"
+                if info["tested"] else "")
+        print(f"calibrate_timesteps: {chosen_text} ({info['status']}), tested from {start_text} on "
+              f"{info['test_grid'][0]}x{info['test_grid'][1]} points in {info['calibration_s']:.2f}s{last}")
+
+    reusable = (info is not None and chosen in info["full_grid_results"] and not args["return_time_trace"]
+                and not args["return_timing_info"])
+    if reusable:
+        result = info["full_grid_results"][chosen]
+        if not np.all(np.isfinite(result)) and not args["ignore_non_finite_output"]:
+            raise RuntimeError("Non-finite values detected in mesolve_2D output. Try reducing dt "
+                               "(increase time samples) or check model parameters/RHS.")
+        if args["return_device"]:
+            import torch
+            return torch.as_tensor(result).cuda()
+        return result
+    finer = False
+    if info is not None:
+        doubling = info["doubling_step_tol"] if adaptive else info["doubling_steps"]
+        finer = doubling < chosen if adaptive else doubling > chosen
+    fallback = info is not None and info["status"] == "converged" and not aligned and finer
+    if fallback:
+        run_args["ignore_non_finite_output"] = True
+    result = _solve_symbolic_system(**run_args)
+    if fallback:
+        values = result[0] if isinstance(result, tuple) else result
+        if not _all_finite(values):
+            new_text = f"step tolerance {doubling:.2e}" if adaptive else f"{doubling} steps"
+            warnings.warn(f"calibrate_timesteps: {chosen_text} passed on the test points but gave non-finite "
+                          f"values on the full grid; using {new_text} instead.", RuntimeWarning, stacklevel=3)
+            chosen = doubling
+            entry["value"] = chosen if adaptive else duration / chosen
+            configure(chosen)
+            run_args["ignore_non_finite_output"] = args["ignore_non_finite_output"]
+            result = _solve_symbolic_system(**run_args)
+    if args["return_timing_info"]:
+        details = {k: v for k, v in info.items() if k != "full_grid_results"} if info else None
+        if adaptive:
+            opts = run_args["adaptive_options"]
+            report = {"step_tol": chosen, "step_rtol": opts["step_rtol"], "step_atol": opts["step_atol"]}
+        else:
+            report = {"steps": chosen, "dt": duration / chosen}
+        result[-1]["timestep_calibration"] = {**report, "calibrated_this_call": info is not None,
+                                              "details": details}
+    return result
+
+
+mesolve_2D.__doc__ = _solve_symbolic_system.__doc__

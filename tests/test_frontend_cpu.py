@@ -1,0 +1,58 @@
+"""CPU tests of the symbolic front end (no GPU): layout, Lindblad equations, emission, options."""
+
+import numpy as np
+import pytest
+import sympy as sp
+
+from gqis import build_independent_rho, build_reduced_lindblad_rhs, compile_lindblad_rhs
+from gqis import emit, rhs as rhs_mod
+from gqis._options import OPTION_GROUPS, apply_option_groups
+
+
+def test_independent_density_matrix_layout():
+    rho, meta = build_independent_rho(3)
+    assert rho.shape == (3, 3)
+    assert len(meta["rho_syms"]) == 8
+    assert meta["num_coherences"] == 3
+    assert sp.simplify(sp.trace(rho) - 1) == 0
+    # Hermitian by construction
+    assert sp.simplify(rho - rho.H) == sp.zeros(3)
+
+
+def test_reduced_lindblad_rhs_matches_two_level_bloch_equations():
+    delta, drive, g1, g2 = sp.symbols("delta drive gamma1 gamma2", real=True, nonnegative=True)
+    sx, sz, sm = sp.Matrix([[0, 1], [1, 0]]), sp.Matrix([[1, 0], [0, -1]]), sp.Matrix([[0, 1], [0, 0]])
+    eqs, mean_re, mean_im, meta = build_reduced_lindblad_rhs(
+        2, delta * sx / 2 + drive * sz / 2, [sp.sqrt(g1) * sm, sp.sqrt(g2) * sz], sp.diag(0, 1))
+    r00, r01re, r01im = meta["rho_syms"]
+    decay = g1 / 2 + 2 * g2
+    expected = [g1 * (1 - r00) - delta * r01im,
+                drive * r01im - decay * r01re,
+                delta * (r00 - sp.Rational(1, 2)) - drive * r01re - decay * r01im]
+    assert all(sp.simplify(a - b) == 0 for a, b in zip(eqs, expected))
+    assert sp.simplify(mean_re - (1 - r00)) == 0 and mean_im == 0
+
+
+def test_emitted_literals_use_ten_significant_digits():
+    eps, A, t, Drive = sp.symbols("eps A t Drive", real=True)
+    c = compile_lindblad_rhs(eps / 2 * sp.Matrix([[1, 0], [0, -1]]) + Drive * sp.Matrix([[0, 1], [1, 0]]),
+                             A * sp.cos(sp.pi * t), [sp.sqrt(0.01) * sp.Matrix([[0, 1], [0, 0]])],
+                             sp.diag(0, 1), [eps, A], RHSreuse=False)
+    frag = emit.emit_model(c, False)
+    assert any("3.141592654e+00" in ln for ln in frag["drive_lines"])
+    assert any("F::cos(" in ln for ln in frag["drive_lines"])
+    assert all("M_PI" not in ln for ln in frag["drive_lines"] + frag["rhs_lines"])
+    assert frag["state_size"] == 3
+
+
+def test_option_groups_merge_and_reject_conflicts():
+    def f(a=1, fp64=False, solver="rk4"):
+        return a
+    args = {"a": 1, "fp64": False, "solver": "rk4"}
+    merged, _ = apply_option_groups(f, dict(args), {"solver_options": {"fp64": True}})
+    assert merged["fp64"] is True
+    with pytest.raises(ValueError, match="both directly"):
+        apply_option_groups(f, dict(args, fp64=True), {"solver_options": {"fp64": False}})
+    with pytest.raises(ValueError, match="Unknown codegen option"):
+        apply_option_groups(f, dict(args), {"codegen": {"fp64": True}})
+    assert "precision" in OPTION_GROUPS["solver_options"]
