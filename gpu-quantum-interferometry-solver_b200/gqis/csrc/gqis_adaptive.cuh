@@ -147,7 +147,7 @@ struct Lane {
     double h, tau;
     int step, substeps, accepted, rejected, next_sample, sample;
     bool rejected_last;
-    typename F::Sum re_sum, im_sum;
+    double re_sum, im_sum;  // trapezoid time average (FP64 in both forms)
     double state_sum[OUT == GQIS_OUT_MEAN_STATE ? S : 1];
     R obs_re_prev, obs_im_prev;
 
@@ -165,8 +165,8 @@ struct Lane {
         next_sample = d.trace_offset;
         sample = 0;
         rejected_last = false;
-        re_sum = typename F::Sum();
-        im_sum = typename F::Sum();
+        re_sum = 0.0;
+        im_sum = 0.0;
         if constexpr (OUT == GQIS_OUT_MEAN_STATE) {
 #pragma unroll
             for (int i = 0; i < S; ++i) state_sum[i] = 0.0;
@@ -201,8 +201,8 @@ struct Lane {
         R* out = static_cast<R*>(d.results);
         const R nan = (R)__longlong_as_double(0x7ff8000000000000LL);
         if constexpr (OUT == GQIS_OUT_MEAN) {
-            out[2 * (size_t)local] = failed ? nan : (R)re_sum.value();
-            out[2 * (size_t)local + 1] = failed ? nan : (R)im_sum.value();
+            out[2 * (size_t)local] = failed ? nan : (R)re_sum;
+            out[2 * (size_t)local + 1] = failed ? nan : (R)im_sum;
         } else if constexpr (OUT == GQIS_OUT_FINAL) {
             R re, im;
             pc.observe(y, Dr, re, im);
@@ -243,8 +243,8 @@ struct Lane {
                 R re, im;
                 pc.observe(y_new, Dr, re, im);
                 if (step >= d.warmup_steps) {
-                    re_sum.add(wgt * ((double)re + (double)obs_re_prev));
-                    im_sum.add(wgt * ((double)im + (double)obs_im_prev));
+                    re_sum = fma(wgt, (double)re + (double)obs_re_prev, re_sum);
+                    im_sum = fma(wgt, (double)im + (double)obs_im_prev, im_sum);
                 }
                 obs_re_prev = re;
                 obs_im_prev = im;

@@ -11,6 +11,12 @@
 #ifndef GQ_BLOCK
 #define GQ_BLOCK 128
 #endif
+#ifndef GQ_MIN_BLOCKS
+#define GQ_MIN_BLOCKS 1
+#endif
+#ifndef GQ_FAST_TRIG
+#define GQ_FAST_TRIG 0
+#endif
 
 // ---------------------------------------------------------------------------------------
 // gq:: math entry points used by the emitted model code. Overloads pick the float or double
@@ -84,14 +90,33 @@ __device__ __forceinline__ float gq_reduce_2pi(double x) {
     return (float)r;
 }
 
+// A step-size coefficient split into a rounded part and its rounding error, so an FP32 form
+// can apply the FP64 value of h/6 (a systematic FP32 rounding of h/6 biases every step).
+template <class R>
+struct Coef {
+    R hi, lo;
+    __device__ __forceinline__ static Coef make(double v) {
+        Coef c;
+        c.hi = (R)v;
+        c.lo = (R)(v - (double)c.hi);
+        return c;
+    }
+};
+
 // Plain FP64 form: the parity form. Everything is double; the time average is a plain
 // running sum as in the reference kernel (N_Level_Kernel.cu:104, gqis/solver.py:2144-2152).
 struct FormFP64 {
     using real = double;
     static constexpr int id = GQIS_FORM_FP64;
+    static constexpr bool kCompensated = false;
     __device__ __forceinline__ static double sin(double x) { return ::sin(x); }
     __device__ __forceinline__ static double cos(double x) { return ::cos(x); }
     __device__ __forceinline__ static double tan(double x) { return ::tan(x); }
+    // y += h * a (c unused)
+    __device__ __forceinline__ static void accumulate(double& y, double& c, double a, Coef<double> h) {
+        (void)c;
+        y = fma(h.hi, a, y);
+    }
     struct Sum {
         double s = 0.0;
         __device__ __forceinline__ void add(double v) { s += v; }
@@ -99,25 +124,51 @@ struct FormFP64 {
     };
 };
 
-// FP32 form: FP32 state, stages and RHS; FP64 time, FP64 drive phase (reduced before the
-// FP32 sin/cos), FP64 compensated (Neumaier) running average.
+// FP32 form: state, stages and RHS in FP32 with three FP64-grade ingredients:
+//  * the state update y += h*a is compensated (Kahan): y carries a running FP32 correction c,
+//    and h is applied as hi + lo, so neither the per-step rounding of y nor a rounded h/6
+//    accumulates over 10^4 steps (without them the map error is ~1e-6, with them ~1e-7);
+//  * time and the drive phase are FP64; the phase is reduced to [-pi, pi] before FP32 sin/cos;
+//  * the running time average is a compensated FP32 sum flushed into FP64 every 256 steps.
 struct FormFP32 {
     using real = float;
     static constexpr int id = GQIS_FORM_FP32;
+    static constexpr bool kCompensated = true;
+#if GQ_FAST_TRIG
+    // Hardware sin/cos on the reduced phase |r| <= pi: absolute error below 2^-21.4.
+    __device__ __forceinline__ static float sin(double x) { return __sinf(gq_reduce_2pi(x)); }
+    __device__ __forceinline__ static float cos(double x) { return __cosf(gq_reduce_2pi(x)); }
+#else
     __device__ __forceinline__ static float sin(double x) { return ::sinf(gq_reduce_2pi(x)); }
     __device__ __forceinline__ static float cos(double x) { return ::cosf(gq_reduce_2pi(x)); }
+#endif
     __device__ __forceinline__ static float tan(double x) { return ::tanf(gq_reduce_2pi(x)); }
     __device__ __forceinline__ static float sin(float x) { return ::sinf(x); }
     __device__ __forceinline__ static float cos(float x) { return ::cosf(x); }
     __device__ __forceinline__ static float tan(float x) { return ::tanf(x); }
+    __device__ __forceinline__ static void accumulate(float& y, float& c, float a, Coef<float> h) {
+        const float d = fmaf(a, h.hi, a * h.lo);  // h * a with h to ~FP64 accuracy, one rounding
+        const float v = d - c;
+        const float s = y + v;
+        c = (s - y) - v;
+        y = s;
+    }
     struct Sum {
-        double s = 0.0, c = 0.0;
-        __device__ __forceinline__ void add(double v) {
-            const double t = s + v;
-            c += (fabs(s) >= fabs(v)) ? ((s - t) + v) : ((v - t) + s);
+        double total = 0.0;
+        float s = 0.0f, c = 0.0f;
+        int n = 0;
+        __device__ __forceinline__ void add(float v) {
+            const float u = v - c;
+            const float t = s + u;
+            c = (t - s) - u;
             s = t;
+            if (++n == 256) {
+                total += (double)s - (double)c;
+                s = c = 0.0f;
+                n = 0;
+            }
         }
-        __device__ __forceinline__ double value() const { return s + c; }
+        __device__ __forceinline__ double value() const { return total + ((double)s - (double)c); }
     };
 };
 
@@ -155,7 +206,7 @@ struct PointCtx {
     }
 
     __device__ __forceinline__ void drives(double t_abs, R* Dr) const {
-        M::template drives<F>(Xd, Yd, t_abs, Dr, Sd, Cd);
+        M::template drives<F>(Xd, Yd, t_abs, X, Y, Dr, Sd, Sr, Cd, Cr);
     }
 
     __device__ __forceinline__ void rhs(const R* y, const R* Dr, R* dy) const {
@@ -209,8 +260,8 @@ struct Recorder {
             if (step_index >= d.warmup_steps) {
                 R re, im;
                 pc.observe(y, Dr, re, im);
-                re_sum.add((double)re);
-                im_sum.add((double)im);
+                re_sum.add(re);
+                im_sum.add(im);
             }
         }
         if constexpr (OUT == GQIS_OUT_MEAN_STATE) {

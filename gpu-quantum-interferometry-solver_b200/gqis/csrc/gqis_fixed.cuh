@@ -14,6 +14,9 @@
 
 namespace gqfixed {
 
+// State updates go through F::accumulate(y, c, a, h): a plain FMA in the FP64 form, a
+// compensated FP32 update (running correction c, h applied as hi + lo) in the FP32 form.
+
 // ------------------------------------------------------------------- classical RK4
 struct RK4 {
     template <class M, class F, int OUT, int TRACE>
@@ -22,14 +25,17 @@ struct RK4 {
         constexpr int S = M::S;
         PointCtx<M, F> pc;
         pc.load(d, p);
-        R y[S], k[S], yt[S], acc[S], Dr[M::NDRV];
+        R y[S], c[S], k[S], yt[S], acc[S], Dr[M::NDRV];
         pc.init(d, local, y);
+#pragma unroll
+        for (int i = 0; i < S; ++i) c[i] = (R)0;
         Recorder<M, F, OUT, TRACE> rec;
         rec.begin(d);
 
         const double dt = d.dt;
         const double dt2d = dt * 0.5;
-        const R h = (R)dt, h2 = (R)dt2d, h6 = (R)(dt / 6.0);
+        const R h = (R)dt, h2 = (R)dt2d;
+        const Coef<R> h6 = Coef<R>::make(dt / 6.0);
         pc.drives(d.t_in + 0.0, Dr);
         pc.rhs(y, Dr, k);
         for (int step = 0; step < d.num_steps; ++step) {
@@ -58,7 +64,7 @@ struct RK4 {
 #pragma unroll
             for (int i = 0; i < S; ++i) {
                 acc[i] += k[i];
-                y[i] = fma(h6, acc[i], y[i]);
+                F::accumulate(y[i], c[i], acc[i], h6);
             }
             if (step + 1 < d.num_steps) pc.rhs(y, Dr, k);
             rec.step(d, pc, local, step, y, Dr);
@@ -79,15 +85,18 @@ struct ExplicitRK {
         constexpr int NS = T::NS;
         PointCtx<M, F> pc;
         pc.load(d, p);
-        R y[S], yt[S], Dr[M::NDRV];
+        R y[S], c[S], yt[S], Dr[M::NDRV];
         R k[NS][S];
         pc.init(d, local, y);
+#pragma unroll
+        for (int i = 0; i < S; ++i) c[i] = (R)0;
         Recorder<M, F, OUT, TRACE> rec;
         rec.begin(d);
 
         const double w = d.solver_params[0];
         const double dt = d.dt;
         const R h = (R)dt;
+        const Coef<R> hc = Coef<R>::make(dt);
         pc.drives(d.t_in + 0.0, Dr);
         pc.rhs(y, Dr, k[0]);
         for (int step = 0; step < d.num_steps; ++step) {
@@ -113,7 +122,7 @@ struct ExplicitRK {
                 for (int j = 0; j < NS; ++j) {
                     if (T::nonzero_b(j)) acc = fma((R)T::b(j, w), k[j][i], acc);
                 }
-                y[i] = fma(h, acc, y[i]);
+                F::accumulate(y[i], c[i], acc, hc);
             }
             if (T::c(NS - 1) != 1.0) pc.drives(d.t_in + (t0 + dt), Dr);
             if (step + 1 < d.num_steps) pc.rhs(y, Dr, k[0]);
@@ -148,8 +157,10 @@ struct LowStorageRK4 {
         constexpr int S = M::S;
         PointCtx<M, F> pc;
         pc.load(d, p);
-        R y[S], k[S], res[S], Dr[M::NDRV];
+        R y[S], c[S], k[S], res[S], Dr[M::NDRV];
         pc.init(d, local, y);
+#pragma unroll
+        for (int i = 0; i < S; ++i) c[i] = (R)0;
         Recorder<M, F, OUT, TRACE> rec;
         rec.begin(d);
         const double dt = d.dt;
@@ -161,10 +172,11 @@ struct LowStorageRK4 {
             for (int s = 0; s < 5; ++s) {
                 if (s > 0) pc.drives(d.t_in + fma(C(s), dt, t0), Dr);
                 pc.rhs(y, Dr, k);
+                const Coef<R> bs = Coef<R>::make(B(s));
 #pragma unroll
                 for (int i = 0; i < S; ++i) {
                     res[i] = (s == 0) ? h * k[i] : fma((R)A(s), res[i], h * k[i]);
-                    y[i] = fma((R)B(s), res[i], y[i]);
+                    F::accumulate(y[i], c[i], res[i], bs);
                 }
             }
             pc.drives(d.t_in + (t0 + dt), Dr);
@@ -183,12 +195,15 @@ struct AdamsBashforth5 {
         PointCtx<M, F> pc;
         pc.load(d, p);
         // f[0] is the newest derivative f_n, f[4] the oldest f_{n-4}.
-        R y[S], yt[S], acc[S], kt[S], f[5][S], Dr[M::NDRV];
+        R y[S], c[S], yt[S], acc[S], kt[S], f[5][S], Dr[M::NDRV];
         pc.init(d, local, y);
+#pragma unroll
+        for (int i = 0; i < S; ++i) c[i] = (R)0;
         Recorder<M, F, OUT, TRACE> rec;
         rec.begin(d);
         const double dt = d.dt;
-        const R h = (R)dt, h2 = (R)(dt * 0.5), h6 = (R)(dt / 6.0);
+        const R h = (R)dt, h2 = (R)(dt * 0.5);
+        const Coef<R> h6 = Coef<R>::make(dt / 6.0), hc = Coef<R>::make(dt);
         pc.drives(d.t_in + 0.0, Dr);
         pc.rhs(y, Dr, f[0]);
         int step = 0;
@@ -217,7 +232,7 @@ struct AdamsBashforth5 {
 #pragma unroll
             for (int i = 0; i < S; ++i) {
                 acc[i] += kt[i];
-                y[i] = fma(h6, acc[i], y[i]);
+                F::accumulate(y[i], c[i], acc[i], h6);
             }
 #pragma unroll
             for (int j = 4; j > 0; --j)
@@ -238,7 +253,7 @@ struct AdamsBashforth5 {
                 s = fma(b2, f[2][i], s);
                 s = fma(b3, f[3][i], s);
                 s = fma(b4, f[4][i], s);
-                y[i] = fma(h, s, y[i]);
+                F::accumulate(y[i], c[i], s, hc);
             }
             pc.drives(d.t_in + (t0 + dt), Dr);
 #pragma unroll
@@ -253,7 +268,7 @@ struct AdamsBashforth5 {
 };
 
 template <class Solver, class M, class F, int OUT, int TRACE>
-__global__ void __launch_bounds__(GQ_BLOCK) sweep_fixed_kernel(const gqis_sweep_desc d) {
+__global__ void __launch_bounds__(GQ_BLOCK, GQ_MIN_BLOCKS) sweep_fixed_kernel(const gqis_sweep_desc d) {
     const int64_t local = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (local >= d.point_count) return;
     Solver::template run<M, F, OUT, TRACE>(d, local, d.point_begin + local);

@@ -30,12 +30,37 @@ _PHASED = ("sin", "cos", "tan")  # periodic functions evaluated through the form
 _MATH_CALL = re.compile(r"(?<![\w:.])(" + "|".join(_MATH) + r")\(")
 
 
-class _ModelPrinter(C99CodePrinter):
-    """C99 printer with ten-digit literals; ``cast=True`` wraps literals as ``R(...)``."""
+PHASE_OPEN, PHASE_CLOSE = "\x01", "\x02"  # marks the FP64 argument of a periodic drive function
 
-    def __init__(self, cast):
+
+class _ModelPrinter(C99CodePrinter):
+    """C99 printer with ten-digit literals; ``cast=True`` wraps literals as ``R(...)``.
+
+    With ``phased=True`` the argument of ``sin``/``cos``/``tan`` is printed in FP64 (plain
+    literals) between the phase markers; ``_phase_names`` later points the symbols inside the
+    markers to their FP64 copies.
+    """
+
+    def __init__(self, cast, phased=False):
         super().__init__()
         self._cast = cast
+        self._phased = phased
+
+    def _print_Function(self, expr):
+        name = expr.func.__name__
+        if self._phased and name in _PHASED and len(expr.args) == 1:
+            inner = _ModelPrinter(cast=False).doprint(expr.args[0])
+            return f"{name}({PHASE_OPEN}{inner}{PHASE_CLOSE})"
+        return super()._print_Function(expr)
+
+    def _print_sin(self, expr):
+        return self._print_Function(expr)
+
+    def _print_cos(self, expr):
+        return self._print_Function(expr)
+
+    def _print_tan(self, expr):
+        return self._print_Function(expr)
 
     def _lit(self, text):
         return f"R({text})" if self._cast else text
@@ -79,14 +104,30 @@ def ccode(expr, *, cast=True, phased=False):
     """Print one expression for the model struct.
 
     ``cast``: literals become ``R(...)`` (arithmetic in the form's type); otherwise they stay
-    FP64. ``phased``: ``sin/cos/tan`` go through ``F::`` (the form's phase-reduced versions).
+    FP64. ``phased``: ``sin/cos/tan`` go through ``F::`` (the form's phase-reduced versions) and
+    their arguments are FP64 (see ``_phase_names``).
     """
-    text = _ModelPrinter(cast).doprint(_evaluate_constants(sp.sympify(expr)))
+    text = _ModelPrinter(cast, phased).doprint(_evaluate_constants(sp.sympify(expr)))
 
     def repl(m):
         name = m.group(1)
         return f"F::{name}(" if phased and name in _PHASED else f"gq::{name}("
     return _MATH_CALL.sub(repl, text)
+
+
+_PHASE_REGION = re.compile(PHASE_OPEN + "(.*?)" + PHASE_CLOSE, re.S)
+
+
+def _phase_names(line):
+    """Inside phase arguments use the FP64 copies of parameters, statics and constants."""
+    def fix(m):
+        body = m.group(1)
+        body = re.sub(r"(?<![\w])ParX(?![\w])", "ParXd", body)
+        body = re.sub(r"(?<![\w])ParY(?![\w])", "ParYd", body)
+        body = body.replace("Static_arr[", "Static_d[").replace("Const_arr[", "Const_d[")
+        body = re.sub(r"(?<![\w])(Drive_arr\[\d+\])", r"((double)\1)", body)
+        return body
+    return _PHASE_REGION.sub(fix, line)
 
 
 def _word(name):
@@ -114,8 +155,8 @@ def emit_model(compiled, uses_rho0_values):
     n_static = 0
     n_drive = len(drive_syms)
 
-    drive_lines += [f"const auto {s} = {ccode(f, cast=False, phased=True)};" for s, f in func_temps]
-    drive_lines += [f"Drive_arr[{k}] = {ccode(e, cast=False, phased=True)};"
+    drive_lines += [f"const R {s} = {ccode(f, cast=True, phased=True)};" for s, f in func_temps]
+    drive_lines += [f"Drive_arr[{k}] = {ccode(e, cast=True, phased=True)};"
                     for k, e in enumerate(drive_exprs)]
 
     def bind(s, e, level):
@@ -126,7 +167,7 @@ def emit_model(compiled, uses_rho0_values):
             names[str(s)] = f"Static_arr[{n_static}]"
             n_static += 1
         else:
-            line = f"Drive_arr[{n_drive}] = {ccode(e, cast=False, phased=True)};"
+            line = f"Drive_arr[{n_drive}] = {ccode(e, cast=True, phased=True)};"
             drive_lines.append(_substitute(line, list(names.items())))
             names[str(s)] = f"Drive_arr[{n_drive}]"
             n_drive += 1
@@ -175,7 +216,7 @@ def emit_model(compiled, uses_rho0_values):
         return out
 
     static_lines = finish(static_lines, False)
-    drive_lines = finish(drive_lines, False)
+    drive_lines = [_phase_names(ln) for ln in finish(drive_lines, True)]
     rhs_lines = finish(rhs_lines, True)
     init_lines = finish(init_lines, False)
     obs_re, obs_im = finish([obs_re, obs_im], True)
@@ -218,12 +259,16 @@ def model_source(frag, struct_name="Model"):
     }}
 
     template <class F>
-    __device__ __forceinline__ static void drives(double ParX, double ParY, double t,
+    __device__ __forceinline__ static void drives(double ParXd, double ParYd, double t,
+                                                  typename F::real ParX, typename F::real ParY,
                                                   typename F::real* __restrict__ Drive_arr,
-                                                  const double* __restrict__ Static_arr,
-                                                  const double* __restrict__ Const_arr) {{
+                                                  const double* __restrict__ Static_d,
+                                                  const typename F::real* __restrict__ Static_arr,
+                                                  const double* __restrict__ Const_d,
+                                                  const typename F::real* __restrict__ Const_arr) {{
         using R = typename F::real;
-        (void)ParX; (void)ParY; (void)t; (void)Drive_arr; (void)Static_arr; (void)Const_arr;
+        (void)ParXd; (void)ParYd; (void)ParX; (void)ParY; (void)t; (void)Drive_arr;
+        (void)Static_d; (void)Static_arr; (void)Const_d; (void)Const_arr;
 {body(frag['drive_lines'])}
     }}
 

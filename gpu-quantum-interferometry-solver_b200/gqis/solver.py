@@ -667,7 +667,7 @@ def _solve_symbolic_system(H, Drive, Col_Ops, mean_operator, tlist,
                 "solver": spec.name, "solver_frequency": solver_frequency, "unroll": unroll,
                 "precision": form, "rhs_flops": emit.count_rhs_flops(frag)}
         module = entry.get("module")
-        if module is not None:
+        if hasattr(module, "info"):
             mi = module.info()
             info.update(registers_per_thread=mi.registers_per_thread, ctas_per_sm=mi.ctas_per_sm,
                         module_path=str(module.path))

@@ -1,0 +1,107 @@
+"""The C ABI on the CPU: header parsing, module build, exported symbols (no compute calls)."""
+
+import ctypes
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+import sympy as sp
+
+from gqis import abi, engine, solver
+from gqis.cuda_solvers import available_solvers, get_solver_spec, normalize_solver_name
+
+HEADER = Path(engine.INCLUDE_DIR) / "gqis_b200.h"
+
+
+def _module_path():
+    t, a, Drive = sp.symbols("t a Drive", real=True)
+    return solver.prebuild("mesolve_2D", sp.Matrix([[a, Drive], [Drive, -a]]) / 2, sp.cos(t),
+                           [sp.Matrix([[0, 0.1], [0, 0]])], sp.diag(0, 1), np.linspace(0, 1, 11),
+                           var_arrays={a: np.linspace(-1, 1, 3)})
+
+
+def test_header_declares_the_module_entry_points():
+    declared = set(abi.header_symbols(HEADER.read_text()))
+    assert set(abi.MODULE_SYMBOLS) <= declared
+
+
+def test_model_module_builds_loads_and_exports_every_declared_symbol():
+    path = _module_path()
+    lib = ctypes.CDLL(str(path))  # loading needs no GPU; no entry point is called here
+    for name in abi.header_symbols(HEADER.read_text()):
+        if name in abi.MODULE_SYMBOLS:
+            assert hasattr(lib, name), name
+    out = subprocess.run(["nm", "-D", "--defined-only", str(path)], capture_output=True, text=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if " T " in line}
+    assert set(abi.MODULE_SYMBOLS) <= exported
+    assert not any(s.startswith("_ZN") and "gqfixed" in s for s in exported)  # templates stay hidden
+
+
+def _struct_fields(text, name):
+    import re
+    body = text[text.index(f"typedef struct {name}"):text.index(f"}} {name};")]
+    body = re.sub(r"/\*.*?\*/", "", body, flags=re.S).split("{", 1)[1]
+    fields = []
+    for decl in body.split(";"):
+        decl = decl.strip()
+        if not decl:
+            continue
+        decl = re.sub(r"\[\d+\]", "", decl)
+        head, *rest = decl.split(",")
+        fields.append(head.replace("*", " ").split()[-1])
+        fields += [r.strip().lstrip("*") for r in rest]
+    return fields
+
+
+def test_descriptor_layout_matches_header_order():
+    text = HEADER.read_text()
+    assert _struct_fields(text, "gqis_sweep_desc") == [f for f, _ in abi.SweepDesc._fields_]
+    assert _struct_fields(text, "gqis_model_info") == [f for f, _ in abi.ModelInfo._fields_]
+    # The C compiler's layout (sizes and every offset) equals the ctypes mirror.
+    prog = ['#include <stdio.h>', '#include <stddef.h>', '#include "gqis_b200.h"', "int main(void) {"]
+    for struct, mirror in (("gqis_sweep_desc", abi.SweepDesc), ("gqis_model_info", abi.ModelInfo)):
+        prog.append(f'printf("%zu\\n", sizeof({struct}));')
+        prog += [f'printf("%zu\\n", offsetof({struct}, {f}));' for f, _ in mirror._fields_]
+    prog.append("return 0; }")
+    import tempfile
+    with tempfile.TemporaryDirectory() as tmp:
+        src, exe = Path(tmp) / "layout.c", Path(tmp) / "layout"
+        src.write_text("\n".join(prog))
+        subprocess.run(["gcc", f"-I{HEADER.parent}", str(src), "-o", str(exe)], check=True)
+        got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()]
+    want = []
+    for mirror in (abi.SweepDesc, abi.ModelInfo):
+        want.append(ctypes.sizeof(mirror))
+        want += [getattr(mirror, f).offset for f, _ in mirror._fields_]
+    assert got == want
+
+
+def test_solver_names_and_aliases():
+    assert available_solvers() == ("rk4", "lserk4", "lserk4f", "dp5", "ab5", "anas5", "tsit5", "alshina6",
+                                   "dop853", "tsit5a", "dop853a")
+    assert normalize_solver_name("RK45") == "dp5"
+    assert normalize_solver_name("Anastassi-Simos") == "anas5"
+    assert normalize_solver_name("DOP-853") == "dop853"
+    assert normalize_solver_name("adaptive_dop853") == "dop853a"
+    with pytest.raises(ValueError, match="Unsupported solver"):
+        normalize_solver_name("not_a_solver")
+
+
+def test_solver_orders_rhs_counts_and_tableaus():
+    assert get_solver_spec("rk4").rhs_evaluations == 4
+    assert get_solver_spec("dop853").rhs_evaluations == 12
+    assert get_solver_spec("ab5").rhs_evaluations == 1
+    for name in ("dp5", "tsit5", "alshina6", "dop853"):
+        t = get_solver_spec(name).tableau
+        assert abs(sum(t.b) - 1.0) < 1e-12, name                     # consistency
+        for i, row in enumerate(t.a):
+            assert abs(sum(row) - t.c[i]) < 1e-10, (name, i)         # row sums = nodes
+    anas = get_solver_spec("anas5", frequency=1.14, step_size=0.01)
+    assert len(anas.parameters) == 1
+    spec = get_solver_spec("tsit5a", step_size=0.1, adaptive_options={"step_rtol": 1e-6})
+    assert spec.parameters[:3] == (1e-6, 1e-5, 64.0)
+    with pytest.raises(ValueError, match="only to the adaptive solvers"):
+        get_solver_spec("tsit5", step_size=0.1, adaptive_options={"step_rtol": 1e-6})
+    with pytest.raises(ValueError, match="Unknown adaptive_options"):
+        get_solver_spec("tsit5a", adaptive_options={"rtol": 1e-6})

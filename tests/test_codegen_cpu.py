@@ -1,0 +1,278 @@
+"""Code generation, caching, validation and API behaviour on the CPU (fake device seam).
+
+Modelled on the reference's CPU tests (``tests/test_ode_api.py``, ``tests/test_package.py``):
+the generated model-module source is inspected instead of launching it.
+"""
+
+import unittest
+import warnings
+from unittest.mock import patch
+
+import numpy as np
+import sympy as sp
+
+import gqis.solver as core
+from gqis import compile_lindblad_rhs, compile_ode_rhs, mesolve_2D, odesolve_2D
+from fake_device import fake_device
+
+
+class OdeApiTests(unittest.TestCase):
+    def setUp(self):
+        self.x, self.y, self.t, self.a = sp.symbols("x y t a", real=True)
+        cm = fake_device()
+        self.dev = cm.__enter__()
+        self.addCleanup(cm.__exit__, None, None, None)
+
+    @property
+    def codes(self):
+        return self.dev.sources
+
+    def solve(self, **kwargs):
+        return odesolve_2D([self.y, -self.a * self.x + sp.sin(self.t)], [self.x, self.y], [1, 0],
+                           np.linspace(0, 1, 9), var_arrays={self.a: np.array([1., 2.])}, **kwargs)
+
+    def test_shapes_and_time_dependent_rhs(self):
+        final, trace, times = self.solve(return_time_trace=True, time_trace_every=3)
+        self.assertEqual(final.shape, (2, 1, 2))
+        self.assertEqual(trace.shape, (2, 1, 3, 2))
+        np.testing.assert_allclose(times, [0.125, 0.5, 0.875])
+        code = self.codes[-1]
+        self.assertIn("static constexpr int S = 2;", code)
+        rhs = code.split("static void rhs(")[1].split("static void observe(")[0]
+        self.assertNotIn("sin(", rhs)  # evaluated in the stage-drive function
+        self.assertIn("F::sin(", code.split("static void drives(")[1].split("static void rhs(")[0])
+        self.assertNotIn("ode_stage_time", code)
+        self.assertIn("#define GQ_TRACE 2", code)  # state trace
+
+    def test_mean_and_shared_rhs(self):
+        mean = self.solve(output_mode="mean")
+        self.assertEqual(mean.shape, (2, 1, 2))
+        self.assertIn("#define GQ_OUT 3", self.codes[-1])  # mean_state
+        count = len(core._RHS_CODE_CACHE)
+        self.solve(solver="tsit5")
+        self.assertEqual(len(core._RHS_CODE_CACHE), count)
+        self.assertIn("ExplicitRK<gqmodel::Tableau>", self.codes[-1])
+
+    def test_time_offset_reuses_kernel_and_shifts_trace_times(self):
+        _, _, times = self.solve(t_in=3.0, return_time_trace=True)
+        np.testing.assert_allclose(times, 3 + np.arange(1, 9) / 8)
+        self.solve(t_in=5.0, return_time_trace=True)
+        self.assertEqual(len(self.codes), 1)
+        self.assertEqual(self.dev.launches[-1].t_in, 5.0)
+
+    def test_observable_and_fp64(self):
+        result, trace, times = self.solve(observable=(self.x + self.y)**2 + sp.I * (self.x + self.y)**3 + self.t,
+                                          fp64=True, return_time_trace=True)
+        self.assertEqual(result.dtype, np.complex128)
+        self.assertEqual(trace.shape, (2, 1, 8))
+        self.assertEqual(times.dtype, np.float64)
+        drives = self.codes[-1].split("static void drives(")[1].split("static void rhs(")[0]
+        self.assertNotIn("rho[", drives)
+        self.assertIn("#define GQ_FORM FormFP64", self.codes[-1])
+
+    def test_fp32_form_is_the_default(self):
+        result = self.solve()
+        self.assertEqual(result.dtype, np.float32)
+        self.assertIn("#define GQ_FORM FormFP32", self.codes[-1])
+
+    def test_static_precomputation(self):
+        odesolve_2D([sp.exp(self.a) * self.x], [self.x], [1], [0, 0.1], var_arrays={self.a: np.array([1.])})
+        static = self.codes[-1].split("static void statics(")[1].split("static void drives(")[0]
+        self.assertIn("gq::exp(ParX)", static)
+
+    def test_explicit_initial_states_and_equations(self):
+        equation = sp.Eq(sp.Derivative(self.x, self.t, evaluate=False), -self.x)
+        result = odesolve_2D([equation], [self.x], None, [0, 0.1], y0_values=np.ones((1, 1)))
+        self.assertEqual(result.shape, (1, 1, 1))
+        self.assertIn("kInitFromArray = true", self.codes[-1])
+
+    def test_invalid_input(self):
+        with self.assertRaisesRegex(ValueError, "Unassigned"):
+            odesolve_2D([self.a * self.x], [self.x], [1], [0, 1])
+        with self.assertRaisesRegex(ValueError, "real"):
+            odesolve_2D([sp.I * self.x], [self.x], [1], [0, 1])
+
+    def test_lindblad_entry_point_still_generates(self):
+        result = mesolve_2D(sp.zeros(2), {}, [], sp.diag(1, 0), [0, 0.1], var_arrays={self.a: np.array([0.])})
+        self.assertEqual(result.shape, (1, 1))
+        self.assertIn("static constexpr int S = 3;", self.codes[-1])
+
+    def test_square_of_a_sum_keeps_its_parentheses(self):
+        odesolve_2D([self.y, -(self.x + 1)**2 - self.a * self.y], [self.x, self.y], [1, 0], [0, 0.1],
+                    var_arrays={self.a: np.array([1.])}, cse_simplify=False)
+        rhs = self.codes[-1].split("static void rhs(")[1].split("static void observe(")[0]
+        self.assertIn("((rho[0] + 1)*(rho[0] + 1))", rhs)
+        self.assertNotIn("pow(", rhs)
+
+    def test_cubes_print_as_products(self):
+        odesolve_2D([self.y, -self.x**3], [self.x, self.y], [1, 0], [0, 0.1], var_arrays={self.a: np.array([1.])})
+        self.assertIn("gq::ipow<3>(rho[0])", self.codes[-1])
+
+    def test_exact_constants_print_as_float_literals(self):
+        odesolve_2D([self.y, -sp.sqrt(2) * self.x - sp.pi * self.a * self.y + sp.E * sp.cos(2 * sp.pi * self.t)],
+                    [self.x, self.y], [1, 0], [0, 0.1], var_arrays={self.a: np.array([1.])})
+        self.assertNotRegex(self.codes[-1], r"\bM_\w+")
+        self.assertIn("1.414213562e+00", self.codes[-1])
+
+    def test_compiled_ode_rhs_starts_from_code_emission(self):
+        compiled = compile_ode_rhs([self.y, -self.a * self.x + sp.sin(self.t)], [self.x, self.y], [1, 0], [self.a])
+        self.assertEqual(set(compiled.timings), {"ode_prepare_s", "ode_optimize_s"})
+        self.assertEqual(self.codes, [])
+        core._RHS_CODE_CACHE.clear()
+        with patch.object(core, "_compile_rhs", side_effect=AssertionError("ODE prepared again")):
+            via = odesolve_2D(compiled, tlist=np.linspace(0, 1, 9), var_arrays={self.a: np.array([1., 2.])})
+        self.assertEqual(via.shape, (2, 1, 2))
+        self.solve()
+        self.assertEqual(len(self.codes), 1)
+        core._KERNEL_CACHE.clear()
+        self.solve()
+        self.assertEqual(self.codes[0], self.codes[1])
+        with self.assertRaisesRegex(ValueError, "var_arrays must sweep"):
+            odesolve_2D(compiled, tlist=[0, 1], var_arrays={})
+        with self.assertRaisesRegex(ValueError, "fixed when the RHS is compiled"):
+            odesolve_2D(compiled, tlist=[0, 1], var_arrays={self.a: np.array([1.])}, observable=self.x)
+        with self.assertRaisesRegex(ValueError, "mesolve_2D"):
+            odesolve_2D(compile_lindblad_rhs(sp.zeros(2), {}, [], sp.diag(1, 0), [self.a]),
+                        tlist=[0, 1], var_arrays={self.a: np.array([0.])})
+
+    def test_compiled_lindblad_rhs_matches_direct_call(self):
+        model = (sp.Matrix([[self.a, 1], [1, -self.a]]), {}, [sp.Matrix([[0, 1], [0, 0]])], sp.diag(1, 0))
+        compiled = compile_lindblad_rhs(*model, [self.a])
+        mesolve_2D(compiled, tlist=[0, 0.1], var_arrays={self.a: np.array([0.])})
+        mesolve_2D(*model, [0, 0.1], var_arrays={self.a: np.array([0.])}, RHSreuse=False)
+        self.assertEqual(self.codes[0], self.codes[1])
+        with self.assertRaisesRegex(ValueError, "order given when the RHS was compiled"):
+            mesolve_2D(compiled, tlist=[0, 0.1], var_arrays={self.x: np.array([0.])})
+        with self.assertRaisesRegex(ValueError, "do not pass the model"):
+            mesolve_2D(compiled, {}, tlist=[0, 0.1], var_arrays={self.a: np.array([0.])})
+
+    def test_grouped_options_match_flat_options(self):
+        flat = self.solve(solver="tsit5", fp64=True, return_time_trace=True, time_trace_every=3, cse_batch_size=1)
+        grouped = self.solve(solver_options={"solver": "tsit5", "fp64": True}, codegen={"cse_batch_size": 1},
+                             output={"return_time_trace": True, "time_trace_every": 3})
+        self.assertEqual(len(self.codes), 1)
+        for a, b in zip(flat, grouped):
+            np.testing.assert_array_equal(a, b)
+
+    def test_grouped_options_reject_conflicts_and_unknown_names(self):
+        with self.assertRaisesRegex(ValueError, "both directly"):
+            self.solve(fp64=True, solver_options={"fp64": False})
+        with self.assertRaisesRegex(ValueError, "Unknown codegen option"):
+            self.solve(codegen={"fp64": True})
+        with self.assertRaisesRegex(ValueError, "does not accept"):
+            mesolve_2D(sp.zeros(2), {}, [], sp.diag(1, 0), [0, 0.1], var_arrays={self.a: np.array([0.])},
+                       initial={"y0_values": None})
+
+    def test_adaptive_solvers_pass_tolerances_and_use_work_stealing_kernel(self):
+        self.solve(solver="dop853a", adaptive_options={"step_rtol": 1e-8, "step_atol": 1e-10, "max_substeps": 99})
+        launch = self.dev.launches[-1]
+        self.assertTrue(launch.adaptive)
+        self.assertEqual(launch.solver_params, (1e-8, 1e-10, 99.0))
+        self.assertIn("Dop853Pair", self.codes[-1])
+        self.assertIn("#define GQ_ADAPTIVE 1", self.codes[-1])
+
+    def test_timestep_calibration_reuse_and_recalibration(self):
+        with patch.object(core, "_calibrate_timestep", wraps=core._calibrate_timestep) as calibrate:
+            settings = dict(rms_atol=1e-4, sample_stride=2)
+            self.solve(calibrate_timesteps=settings)
+            self.solve(calibrate_timesteps=settings)
+            self.assertEqual(calibrate.call_count, 1)
+            self.solve(calibrate_timesteps=settings, cse_batch_size=1)
+            self.assertEqual(calibrate.call_count, 1)
+            self.solve(calibrate_timesteps=dict(settings, rms_atol=1e-5))
+            self.assertEqual(calibrate.call_count, 2)
+            every = dict(settings, recalibrate_every=2, max_atol=0)
+            for _ in range(3):
+                self.solve(calibrate_timesteps=every)
+            self.assertEqual(calibrate.call_count, 4)
+            self.solve(calibrate_timesteps=dict(every, reset=True))
+            self.assertEqual(calibrate.call_count, 5)
+
+    def test_timestep_calibration_never_accepts_unstable_runs(self):
+        def fake_solve(**kwargs):
+            steps = len(kwargs["tlist"]) - 1
+            return np.full((2, 2), np.nan) if steps < 4 else np.ones((2, 2))
+        args = dict(var_arrays={self.a: np.arange(10.)}, rho0_var_arrays=None, rho0_values=None,
+                    solver="rk4", fp64=False)
+        settings = core._timestep_calibration_settings(dict(rms_atol=0, max_atol=0, rms_rtol=1e-3))
+        with patch.object(core, "_solve_symbolic_system", fake_solve):
+            info = core._calibrate_timestep(args, settings, base_steps=1, duration=1.0)
+        self.assertEqual(info["steps"], 4)
+
+    def test_timestep_calibration_test_grid_keeps_axis_ends(self):
+        args = dict(var_arrays={self.a: np.arange(10.)}, rho0_var_arrays=None, rho0_values=np.zeros((10, 3)),
+                    solver="rk4", fp64=False)
+        test, full_grid = core._undersampled_arguments(args, 4)
+        np.testing.assert_array_equal(test["var_arrays"][self.a], [0, 4, 8, 9])
+        self.assertEqual(test["rho0_values"].shape, (4, 3))
+        self.assertFalse(full_grid)
+        self.assertTrue(core._undersampled_arguments(args, 1)[1])
+
+    def test_timestep_calibration_warns_once_for_wider_sweep_range(self):
+        settings = dict(rms_atol=1e-4, sample_stride=2)
+        self.solve(calibrate_timesteps=settings)
+        wider = dict(var_arrays={self.a: np.array([1., 3.])})
+        model = ([self.y, -self.a * self.x + sp.sin(self.t)], [self.x, self.y], [1, 0], np.linspace(0, 1, 9))
+        with self.assertWarnsRegex(RuntimeWarning, "beyond the range used for calibration"):
+            odesolve_2D(*model, calibrate_timesteps=settings, **wider)
+        with warnings.catch_warnings():
+            warnings.simplefilter("error")
+            odesolve_2D(*model, calibrate_timesteps=settings, **wider)
+
+    def test_timestep_calibration_bisection_finds_coarsest_passing_step(self):
+        real = core._solve_symbolic_system
+
+        def fake(**kwargs):
+            if kwargs.get("calibrate_timesteps"):
+                return real(**kwargs)
+            steps = len(kwargs["tlist"]) - 1
+            shape = tuple(len(v) for v in kwargs["var_arrays"].values()) + (1,)
+            result = np.full(shape[:2], 0.3 + 3e4 / steps**4, dtype=complex)
+            return (result, {}) if kwargs.get("return_timing_info") else result
+
+        def steps_for(start, bisection_steps):
+            core._TIMESTEP_CALIBRATION_CACHE.clear()
+            with patch.object(core, "_solve_symbolic_system", side_effect=fake):
+                _, info = real(H=sp.eye(2), Drive=sp.Integer(0), Col_Ops=[], mean_operator=sp.eye(2),
+                               tlist=np.linspace(0, 1, start + 1), var_arrays={self.a: np.ones(4)},
+                               return_timing_info=True, output_mode="final",
+                               calibrate_timesteps=dict(rms_atol=1e-3, max_atol=1e-2,
+                                                        bisection_steps=bisection_steps))
+            return info["timestep_calibration"]["steps"]
+
+        self.assertEqual(steps_for(16, 0), 128)
+        self.assertEqual(steps_for(16, 2), 76)
+        self.assertEqual(steps_for(512, 2), 76)
+        self.assertEqual(steps_for(512, 0), 512)
+
+    def test_timestep_calibration_defaults_differ_for_lindblad_and_ode(self):
+        lindblad = core._timestep_calibration_settings(True)
+        ode = core._timestep_calibration_settings(True, ode=True)
+        self.assertEqual((lindblad["rms_atol"], lindblad["max_atol"]), (1e-3, 1e-2))
+        self.assertEqual((ode["rms_atol"], ode["max_atol"]), (1e-4, 1e-3))
+
+    def test_timestep_calibration_rejects_unknown_settings(self):
+        with self.assertRaisesRegex(ValueError, "Unknown calibrate_timesteps"):
+            self.solve(calibrate_timesteps=dict(rms_tol=1e-4))
+        with self.assertRaisesRegex(ValueError, "at least one"):
+            self.solve(calibrate_timesteps=dict(rms_atol=0, max_atol=0))
+
+
+def _minimal_model():
+    sweep = sp.Symbol("sweep", real=True)
+    return sp.zeros(2), sp.Integer(0), [], sp.eye(2), {sweep: np.array([0.0])}
+
+
+def test_nonuniform_time_grid_is_rejected_before_gpu_launch():
+    import pytest
+    H, D, C, O, sweep = _minimal_model()
+    with pytest.raises(ValueError, match="uniformly spaced"):
+        mesolve_2D(H, D, C, O, [0.0, 1.0, 2.5], var_arrays=sweep)
+    with pytest.raises(ValueError, match="begin at zero"):
+        mesolve_2D(H, D, C, O, [1.0, 2.0], var_arrays=sweep)
+    with pytest.raises(ValueError, match="Unsupported solver"):
+        mesolve_2D(H, D, C, O, [0.0, 1.0], var_arrays=sweep, solver="not_a_solver")
+    with pytest.raises(ValueError, match="unroll must be True or False"):
+        mesolve_2D(H, D, C, O, [0.0, 1.0], var_arrays=sweep, unroll="False")
+    with pytest.raises(ValueError, match="precision must be"):
+        mesolve_2D(H, D, C, O, [0.0, 1.0], var_arrays=sweep, precision="bf16")
