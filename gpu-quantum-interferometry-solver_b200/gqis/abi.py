@@ -37,7 +37,7 @@ class SweepDesc(ctypes.Structure):
                 ("solver_params", ctypes.c_double * 8)]
 
 
-MODULE_SYMBOLS = ("gqis_model_info_get", "gqis_sweep_launch", "gqis_last_error")
+MODULE_SYMBOLS = ("gqis_model_info_get", "gqis_sweep_launch", "gqis_last_error", "gqis_sweep_launch_noalloc")
 
 
 def bind_module(lib):
@@ -46,6 +46,8 @@ def bind_module(lib):
     lib.gqis_model_info_get.restype = ctypes.c_int
     lib.gqis_sweep_launch.argtypes = [ctypes.POINTER(SweepDesc), ctypes.c_void_p]
     lib.gqis_sweep_launch.restype = ctypes.c_int
+    lib.gqis_sweep_launch_noalloc.argtypes = [ctypes.POINTER(SweepDesc), ctypes.c_void_p]
+    lib.gqis_sweep_launch_noalloc.restype = ctypes.c_int
     lib.gqis_last_error.argtypes = []
     lib.gqis_last_error.restype = ctypes.c_char_p
 

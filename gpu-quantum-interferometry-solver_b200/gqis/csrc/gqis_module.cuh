@@ -13,6 +13,8 @@
 #include <stdarg.h>
 #include <stdio.h>
 
+#include <mutex>
+
 #include "gqis_fixed.cuh"
 #include "gqis_adaptive.cuh"
 
@@ -136,6 +138,76 @@ __attribute__((visibility("default"))) int gqis_sweep_launch(const gqis_sweep_de
     cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) return cuda_fail(err, "sweep kernel launch");
     return GQIS_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------
+// Allocation-free launch (gqis_sweep_launch_noalloc): the adaptive kernels' work counter lives
+// in this file-scope device array instead of caller-provided scratch. Host code only ever
+// uses the array's device address, looked up once per device with cudaGetSymbolAddress.
+// ---------------------------------------------------------------------------------------
+static __device__ __align__(256) unsigned int g_noalloc_scratch[GQIS_NOALLOC_SCRATCH_BYTES / sizeof(unsigned int)];
+
+namespace {
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+unsigned int* g_noalloc_address[kNoallocMaxDevices] = {};
+
+int noalloc_scratch_address(unsigned int** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    if (dev < 0 || dev >= kNoallocMaxDevices)
+        return fail(GQIS_ERR_UNSUPPORTED, "device %d is beyond the %d devices the no-alloc launch tracks", dev,
+                    kNoallocMaxDevices);
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_address[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+        g_noalloc_address[dev] = static_cast<unsigned int*>(p);
+    }
+    *out = g_noalloc_address[dev];
+    return GQIS_OK;
+}
+}  // namespace
+
+extern "C" {
+
+__attribute__((visibility("default"))) int gqis_sweep_launch_noalloc(const gqis_sweep_desc* d, void* stream) {
+#if GQ_ADAPTIVE
+    if (!d) return fail(GQIS_ERR_INVALID, "descriptor is NULL");
+    if (d->point_count > GQIS_NOALLOC_MAX_POINTS)
+        return fail(GQIS_ERR_TOO_LARGE, "no-alloc launch: %lld points exceed the maximum of %lld per call",
+                    (long long)d->point_count, (long long)GQIS_NOALLOC_MAX_POINTS);
+    unsigned int* counter = nullptr;
+    int rc = noalloc_scratch_address(&counter);
+    if (rc != GQIS_OK) return rc;
+    gqis_sweep_desc local = *d;
+    local.work_counter = counter;
+    rc = check_desc(&local);
+    if (rc != GQIS_OK || local.point_count == 0) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), st);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(no-alloc work counter)");
+    int dev = 0, sms = 0, ctas = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+        return cuda_fail(e, "cudaDeviceGetAttribute");
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas, kKernel, GQ_BLOCK, 0)) != cudaSuccess)
+        return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    if (ctas < 1) ctas = 1;
+    const int64_t needed = (local.point_count + GQ_BLOCK - 1) / GQ_BLOCK;
+    int64_t grid = (int64_t)sms * ctas;
+    if (grid > needed) grid = needed;
+    kKernel<<<(unsigned)grid, GQ_BLOCK, 0, st>>>(local);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "no-alloc sweep kernel launch");
+    return GQIS_OK;
+#else
+    return gqis_sweep_launch(d, stream);  // fixed-step kernels use no scratch
+#endif
 }
 
 }  // extern "C"

@@ -121,6 +121,26 @@ int gqis_sweep_launch(const gqis_sweep_desc* desc, void* stream);
 /* Thread-local text of the last error of this module (never NULL). */
 const char* gqis_last_error(void);
 
+/* No counterpart in the reference: a launch that allocates nothing, for callers that cannot
+ * call cudaMalloc - a host whose caching allocator owns the device memory (a PyTorch or JAX
+ * process near its memory cap), a real-time loop where cudaMalloc/cudaFree would synchronize
+ * the device, a plugin that is handed only its input and output buffers.
+ *
+ * Same as gqis_sweep_launch, except that the adaptive kernels take their scratch - the
+ * work-stealing point counter - from a file-scope device array of this module
+ * (GQIS_NOALLOC_SCRATCH_BYTES, held on every device that loads the module until exit) instead
+ * of desc->work_counter, which is ignored. The caller still passes inputs and outputs.
+ * Fixed-step modules use no scratch and behave exactly like gqis_sweep_launch.
+ *  - At most GQIS_NOALLOC_MAX_POINTS points per call (the counter's range); larger requests
+ *    return GQIS_ERR_TOO_LARGE.
+ *  - The first call on a device looks up the array's device address (once per device, with
+ *    that device current); make that first call before any stream capture.
+ *  - Each call clears the counter on its stream before the kernel. All calls share the one
+ *    array: calls whose kernels overlap on the GPU (other streams, other threads) race. */
+#define GQIS_NOALLOC_SCRATCH_BYTES 256
+#define GQIS_NOALLOC_MAX_POINTS 2147483647LL
+int gqis_sweep_launch_noalloc(const gqis_sweep_desc* desc, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
