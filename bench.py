@@ -288,8 +288,8 @@ def run_ours(args):
             ref = cpu_reference(steps=1, sample="c2_fp64_mean_sub128")
             line["cpu_baseline"] = {"value": ref["points"] * ref["steps"] / ref["times"][0], "unit": UNIT,
                                     "cores": ref["cores"], "kind": ref["kind"], "sample": ref["sample"]}
-        if ws == 1 and args.reference_gpu:
-            line["reference_kernel_gpu"] = reference_gpu_kernels()
+        if ws == 1 and args.reference_gpu and side == SIDE and nsteps == NSTEPS:
+            line["reference_kernel_gpu"] = reference_gpu_kernels(ref_map)
     if ws > 1:
         import torch.distributed as dist
         dist.barrier()
@@ -299,18 +299,23 @@ def run_ours(args):
     return 0
 
 
-def reference_gpu_kernels():
-    """The reference's own generated kernels for this workload, compiled for sm_100a, same GPU."""
+def reference_gpu_kernels(fp64_map):
+    """The reference's own generated kernels for this workload, compiled for sm_100a, same GPU,
+    with each map's max-abs difference from our plain FP64 map (which equals the reference FP64
+    kernel's map to 1e-10)."""
+    import numpy as np
     sys.path.insert(0, str(ROOT / "oracle"))
     import ref_kernels
+    ours = fp64_map[:, 0].cpu().numpy().reshape(SIDE, SIDE)
     out = {}
     for form, case in (("fp64", "c2_fp64_mean_full"), ("fp32", "c2_fp32_mean_full")):
         if not ref_kernels.available(case, "gpu"):
             out[form] = None
             continue
-        ref_kernels.run_case(case, "gpu")
+        res, _ = ref_kernels.run_case(case, "gpu")
         _, dt = ref_kernels.run_case(case, "gpu", repeats=2)
-        out[form] = {"ms_per_sweep": dt * 1e3, "value": SIDE * SIDE * NSTEPS / dt}
+        err = float(np.max(np.abs(res["result"].real - ours)))
+        out[form] = {"ms_per_sweep": dt * 1e3, "value": SIDE * SIDE * NSTEPS / dt, "max_abs_diff_vs_our_fp64": err}
     return out
 
 

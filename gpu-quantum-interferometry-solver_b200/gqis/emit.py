@@ -115,19 +115,19 @@ def ccode(expr, *, cast=True, phased=False):
     return _MATH_CALL.sub(repl, text)
 
 
-_PHASE_REGION = re.compile(PHASE_OPEN + "(.*?)" + PHASE_CLOSE, re.S)
+def _fp64_names(line):
+    """A drive line evaluated entirely in FP64: FP64 copies of every input, results in ``Dd``.
 
-
-def _phase_names(line):
-    """Inside phase arguments use the FP64 copies of parameters, statics and constants."""
-    def fix(m):
-        body = m.group(1)
-        body = re.sub(r"(?<![\w])ParX(?![\w])", "ParXd", body)
-        body = re.sub(r"(?<![\w])ParY(?![\w])", "ParYd", body)
-        body = body.replace("Static_arr[", "Static_d[").replace("Const_arr[", "Const_d[")
-        body = re.sub(r"(?<![\w])(Drive_arr\[\d+\])", r"((double)\1)", body)
-        return body
-    return _PHASE_REGION.sub(fix, line)
+    Rounding a sweep parameter to FP32 before it enters a drive (``eps + A cos(w t)``) shifts
+    the model by a fixed amount at every step, a systematic error that reached 1.5e-6 at sharp
+    resonances of the four-level map; evaluated in FP64 and rounded once per stage time, the
+    drive's rounding varies in time and averages out (5e-8 there).
+    """
+    line = line.replace(PHASE_OPEN, "").replace(PHASE_CLOSE, "")
+    line = re.sub(r"(?<![\w])ParX(?![\w])", "ParXd", line)
+    line = re.sub(r"(?<![\w])ParY(?![\w])", "ParYd", line)
+    line = line.replace("Static_arr[", "Static_d[").replace("Const_arr[", "Const_d[")
+    return line.replace("Drive_arr[", "Dd[")
 
 
 def _word(name):
@@ -155,8 +155,8 @@ def emit_model(compiled, uses_rho0_values):
     n_static = 0
     n_drive = len(drive_syms)
 
-    drive_lines += [f"const R {s} = {ccode(f, cast=True, phased=True)};" for s, f in func_temps]
-    drive_lines += [f"Drive_arr[{k}] = {ccode(e, cast=True, phased=True)};"
+    drive_lines += [f"const double {s} = {ccode(f, cast=False, phased=True)};" for s, f in func_temps]
+    drive_lines += [f"Drive_arr[{k}] = {ccode(e, cast=False, phased=True)};"
                     for k, e in enumerate(drive_exprs)]
 
     def bind(s, e, level):
@@ -167,7 +167,7 @@ def emit_model(compiled, uses_rho0_values):
             names[str(s)] = f"Static_arr[{n_static}]"
             n_static += 1
         else:
-            line = f"Drive_arr[{n_drive}] = {ccode(e, cast=True, phased=True)};"
+            line = f"Drive_arr[{n_drive}] = {ccode(e, cast=False, phased=True)};"
             drive_lines.append(_substitute(line, list(names.items())))
             names[str(s)] = f"Drive_arr[{n_drive}]"
             n_drive += 1
@@ -216,7 +216,7 @@ def emit_model(compiled, uses_rho0_values):
         return out
 
     static_lines = finish(static_lines, False)
-    drive_lines = [_phase_names(ln) for ln in finish(drive_lines, True)]
+    drive_lines = [_fp64_names(ln) for ln in finish(drive_lines, False)]
     rhs_lines = finish(rhs_lines, True)
     init_lines = finish(init_lines, False)
     obs_re, obs_im = finish([obs_re, obs_im], True)
@@ -233,6 +233,7 @@ def emit_model(compiled, uses_rho0_values):
         obs_re, obs_im = renumber(obs_re), renumber(obs_im)
 
     return {"state_size": size, "n_static": max(1, n_static), "n_drive": max(1, n_drive),
+            "n_drive_used": n_drive,
             "n_const": max(1, len(used)), "used_const_indices": tuple(used),
             "static_lines": tuple(static_lines), "drive_lines": tuple(drive_lines),
             "rhs_lines": tuple(rhs_lines), "obs_re": obs_re, "obs_im": obs_im,
@@ -269,7 +270,11 @@ def model_source(frag, struct_name="Model"):
         using R = typename F::real;
         (void)ParXd; (void)ParYd; (void)ParX; (void)ParY; (void)t; (void)Drive_arr;
         (void)Static_d; (void)Static_arr; (void)Const_d; (void)Const_arr;
+        double Dd[NDRV];
+        (void)Dd;
 {body(frag['drive_lines'])}
+#pragma unroll
+        for (int k = 0; k < {frag['n_drive_used']}; ++k) Drive_arr[k] = (R)Dd[k];
     }}
 
     template <class R>
