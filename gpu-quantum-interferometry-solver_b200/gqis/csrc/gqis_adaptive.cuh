@@ -290,6 +290,12 @@ struct Lane {
     }
 };
 
+// GQ_STATIC_SCHEDULE=1 builds the classic one-point-per-thread schedule instead (grid = all
+// points, no refill), kept for measuring what the work stealing gains.
+#ifndef GQ_STATIC_SCHEDULE
+#define GQ_STATIC_SCHEDULE 0
+#endif
+
 template <class Pair, class M, class F, int OUT, int TRACE>
 __global__ void __launch_bounds__(GQ_BLOCK) sweep_adaptive_kernel(const gqis_sweep_desc d) {
     const unsigned lane_id = threadIdx.x & 31u;
@@ -298,6 +304,17 @@ __global__ void __launch_bounds__(GQ_BLOCK) sweep_adaptive_kernel(const gqis_swe
     const double inv_avg_time = 1.0 / ((double)(d.num_steps - d.warmup_steps) * d.dt);
     Lane<Pair, M, F, OUT, TRACE> L;
     bool active = false, exhausted = false;
+#if GQ_STATIC_SCHEDULE
+    {
+        const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+        if (idx < d.point_count) {
+            L.start(d, idx);
+            active = true;
+        }
+        exhausted = true;
+        (void)lane_id;
+    }
+#endif
     for (;;) {
         const unsigned need = __ballot_sync(0xffffffffu, !active && !exhausted);
         if (need) {

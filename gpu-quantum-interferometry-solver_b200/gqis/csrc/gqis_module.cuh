@@ -127,7 +127,7 @@ __attribute__((visibility("default"))) int gqis_sweep_launch(const gqis_sweep_de
         return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
     if (ctas < 1) ctas = 1;
     const int64_t needed = (d->point_count + GQ_BLOCK - 1) / GQ_BLOCK;
-    int64_t grid = (int64_t)sms * ctas;
+    int64_t grid = GQ_STATIC_SCHEDULE ? needed : (int64_t)sms * ctas;
     if (grid > needed) grid = needed;
     kKernel<<<(unsigned)grid, GQ_BLOCK, 0, st>>>(*d);
 #else
@@ -199,7 +199,7 @@ __attribute__((visibility("default"))) int gqis_sweep_launch_noalloc(const gqis_
         return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
     if (ctas < 1) ctas = 1;
     const int64_t needed = (local.point_count + GQ_BLOCK - 1) / GQ_BLOCK;
-    int64_t grid = (int64_t)sms * ctas;
+    int64_t grid = GQ_STATIC_SCHEDULE ? needed : (int64_t)sms * ctas;
     if (grid > needed) grid = needed;
     kKernel<<<(unsigned)grid, GQ_BLOCK, 0, st>>>(local);
     e = cudaGetLastError();
