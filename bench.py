@@ -384,6 +384,74 @@ def run_duffing(args):
     return 0
 
 
+def run_serving(args):
+    """Config C5 (sweeps): Poisson stream of mixed-N, mixed-size sweep requests through the
+    continuous-batching server (FP32 form), against the same requests one by one on plain FP64."""
+    import numpy as np
+    import torch
+    torch.cuda.set_device(0)
+    sys.path.insert(0, str(ROOT / "tests"))
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import gqis
+    from gqis.serving import SweepServer
+    from test_support_calls import SERVING_SIDES, serving_model
+    rng = np.random.default_rng(args.seed)
+    dims = (2, 4, 8)
+    reqs = []
+    t = 0.0
+    for _ in range(args.requests):
+        t += rng.exponential(1.0 / args.rate)
+        N = int(rng.choice(dims))
+        side = int(rng.choice(SERVING_SIDES))
+        reqs.append((t, N, side))
+    models = {}
+    for _, N, side in reqs:
+        if (N, side) not in models:
+            models[(N, side)] = serving_model(N, side)
+    for N in dims:  # warm the caches (symbolic model, module load) before timing
+        a, kw = serving_model(N, 64)
+        gqis.mesolve_2D(*a, **kw, precision="fp32")
+        gqis.mesolve_2D(*a, **kw, precision="fp64")
+    point_steps = sum(side * side * (len(models[(N, side)][0][4]) - 1) for _, N, side in reqs)
+    futs = []
+    with SweepServer(streams=4, chunk_points=1 << 15, max_inflight=16) as srv:
+        t0 = time.perf_counter()
+        for arrival, N, side in reqs:
+            delay = t0 + arrival - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            a, kw = models[(N, side)]
+            futs.append(srv.submit("mesolve_2D", *a, **kw, precision="fp32"))
+        for f in futs:
+            f.result(600)
+        t_end = max(f.finished_at for f in futs)
+        stats = dict(srv.stats)
+    lat = np.array([f.latency for f in futs]) * 1e3
+    served = point_steps / (t_end - t0)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    for _, N, side in reqs:  # the same requests one by one on the plain FP64 path
+        a, kw = models[(N, side)]
+        gqis.mesolve_2D(*a, **kw, precision="fp64")
+    torch.cuda.synchronize()
+    seq = point_steps / (time.perf_counter() - t1)
+    line = {
+        "metric": "sweep serving: aggregate points*steps/s and latency (Poisson 50/s, N in {2,4,8})",
+        "value": served, "unit": "points*steps/s", "n_gpus": 1, "steps": args.requests, "warmup": len(dims),
+        "ms_per_step": float(np.mean(lat)), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{args.requests} seeded requests, Poisson rate {args.rate}/s, N uniform in {dims}, "
+                               f"grid side uniform in {SERVING_SIDES}, mean <O> maps, RK4 (model tlists)",
+                   "server": "4 streams, 32768-point chunks, <= 16 admitted requests, memory budget 50% free"},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                       "max": float(lat.max())},
+        "one_by_one_fp64": {"value": seq}, "speedup_vs_one_by_one_fp64": served / seq,
+        "server_stats": stats, "total_point_steps": point_steps,
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -395,7 +463,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--reference-gpu", action="store_true",
                     help="also time the reference's generated kernels on this GPU")
-    ap.add_argument("--workload", default="four_level", choices=("four_level", "duffing"),
+    ap.add_argument("--requests", type=int, default=48, help="serving: number of requests")
+    ap.add_argument("--rate", type=float, default=50.0, help="serving: Poisson arrival rate (1/s)")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--workload", default="four_level", choices=("four_level", "duffing", "serving"),
                     help="four_level: the headline RK4 interferogram; duffing: the adaptive ODE sweep")
     ap.add_argument("--solver", default="dop853a", help="adaptive solver of --workload duffing")
     args = ap.parse_args()
@@ -403,6 +474,8 @@ def main():
         return run_reference(args)
     if args.workload == "duffing":
         return run_duffing(args)
+    if args.workload == "serving":
+        return run_serving(args)
     return run_ours(args)
 
 

@@ -17,6 +17,11 @@
 
 #include "gqis_fixed.cuh"
 #include "gqis_adaptive.cuh"
+#include "gqis_adjoint.cuh"
+
+#ifndef GQ_WITH_ADJOINT
+#define GQ_WITH_ADJOINT 0
+#endif
 
 namespace {
 
@@ -207,6 +212,66 @@ __attribute__((visibility("default"))) int gqis_sweep_launch_noalloc(const gqis_
     return GQIS_OK;
 #else
     return gqis_sweep_launch(d, stream);  // fixed-step kernels use no scratch
+#endif
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------
+// Adjoint entry points (modules generated with an adjoint struct gqmodel::Adjoint).
+// ---------------------------------------------------------------------------------------
+extern "C" {
+
+__attribute__((visibility("default"))) int gqis_adjoint_info(int32_t* num_params, int32_t* state_size) {
+#if GQ_WITH_ADJOINT
+    if (num_params) *num_params = gqmodel::Adjoint::P;
+    if (state_size) *state_size = Model::S;
+    return GQIS_OK;
+#else
+    (void)num_params;
+    (void)state_size;
+    return fail(GQIS_ERR_UNSUPPORTED, "this module was built without an adjoint");
+#endif
+}
+
+__attribute__((visibility("default"))) int gqis_adjoint_scratch_bytes(int64_t point_count, int32_t num_steps,
+                                                                       int32_t checkpoint_every, int64_t* bytes) {
+    if (!bytes || point_count < 0 || num_steps < 1 || checkpoint_every < 1)
+        return fail(GQIS_ERR_INVALID, "adjoint scratch: invalid sizes");
+    const int64_t nck = (num_steps + checkpoint_every - 1) / checkpoint_every;
+    *bytes = (nck + checkpoint_every) * (int64_t)Model::S * point_count * (int64_t)sizeof(double);
+    return GQIS_OK;
+}
+
+__attribute__((visibility("default"))) int gqis_adjoint_launch(const gqis_adjoint_desc* a, void* stream) {
+#if GQ_WITH_ADJOINT
+    if (!a) return fail(GQIS_ERR_INVALID, "adjoint descriptor is NULL");
+    if (Form::id != GQIS_FORM_FP64) return fail(GQIS_ERR_UNSUPPORTED, "the adjoint runs in the FP64 form");
+    int rc = check_desc(&a->sweep);
+    if (rc != GQIS_OK) return rc;
+    if (a->sweep.warmup_steps >= a->sweep.num_steps)
+        return fail(GQIS_ERR_INVALID, "the adjoint differentiates a mean: needs steps after warmup");
+    if (a->num_params != gqmodel::Adjoint::P)
+        return fail(GQIS_ERR_INVALID, "num_params %d, module has %d", a->num_params, gqmodel::Adjoint::P);
+    if (a->checkpoint_every < 1) return fail(GQIS_ERR_INVALID, "checkpoint_every must be positive");
+    int64_t need = 0;
+    rc = gqis_adjoint_scratch_bytes(a->sweep.point_count, a->sweep.num_steps, a->checkpoint_every, &need);
+    if (rc != GQIS_OK) return rc;
+    if (!a->scratch || a->scratch_bytes < need)
+        return fail(GQIS_ERR_INVALID, "adjoint scratch of %lld bytes needed, %lld given", (long long)need,
+                    (long long)a->scratch_bytes);
+    if (gqmodel::Adjoint::P > 0 && !a->grad) return fail(GQIS_ERR_INVALID, "grad buffer is NULL");
+    if (a->sweep.point_count == 0) return GQIS_OK;
+    const int64_t grid = (a->sweep.point_count + GQ_BLOCK - 1) / GQ_BLOCK;
+    gqadjoint::adjoint_rk4_kernel<Model, gqmodel::Adjoint>
+        <<<(unsigned)grid, GQ_BLOCK, 0, static_cast<cudaStream_t>(stream)>>>(*a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "adjoint kernel launch");
+    return GQIS_OK;
+#else
+    (void)a;
+    (void)stream;
+    return fail(GQIS_ERR_UNSUPPORTED, "this module was built without an adjoint");
 #endif
 }
 

@@ -17,6 +17,9 @@ code. ``emit.py`` turns its plan into the model functions the CUDA templates cal
 
 from __future__ import annotations
 
+import hashlib
+import os
+import pickle
 import time
 from dataclasses import dataclass, field
 
@@ -346,6 +349,11 @@ def compile_rhs(H, Drive, Col_Ops, mean_operator, *, sweep_symbols, const_values
            pre_expand, collect_rho, factor_terms, cse_batch_size, cse_simplify, hoist_rho_independent)
     if reuse and key in _RHS_CODE_CACHE:
         return _RHS_CODE_CACHE[key], "hit"
+    if reuse:
+        stored = _disk_get(key)
+        if stored is not None:
+            _RHS_CODE_CACHE[key] = stored
+            return stored, "hit"
 
     size = model["state_size"]
     if ode_size is None:
@@ -380,7 +388,53 @@ def compile_rhs(H, Drive, Col_Ops, mean_operator, *, sweep_symbols, const_values
         model=model)
     if reuse:
         _RHS_CODE_CACHE[key] = compiled
+        _disk_put(key, compiled)
     return compiled, "miss"
+
+
+# ----------------------------------------------------------------------------------------
+# persistent cache of prepared RHS objects
+# ----------------------------------------------------------------------------------------
+# The symbolic derivation of larger models takes tens of seconds (N = 8: ~30 s) and, like the
+# reference (which recompiles per process), would repeat in every new process. Prepared
+# CompiledRHS objects are therefore pickled next to the model modules, keyed by the structural
+# cache key. GQIS_DISK_CACHE=0 disables it.
+
+def _disk_path(key):
+    from .engine import cache_dir
+    digest = hashlib.sha256(repr(key).encode()).hexdigest()[:32]
+    return cache_dir().parent / "rhs" / f"{digest}.pkl"
+
+
+def _disk_get(key):
+    if os.environ.get("GQIS_DISK_CACHE", "1") == "0":
+        return None
+    path = _disk_path(key)
+    if not path.exists():
+        return None
+    try:
+        with open(path, "rb") as f:
+            stored_key, compiled = pickle.load(f)
+    except Exception:
+        return None
+    if stored_key != key:
+        return None
+    compiled.emitted = {}
+    return compiled
+
+
+def _disk_put(key, compiled):
+    if os.environ.get("GQIS_DISK_CACHE", "1") == "0":
+        return
+    path = _disk_path(key)
+    try:
+        path.parent.mkdir(parents=True, exist_ok=True)
+        tmp = path.with_suffix(f".{os.getpid()}.tmp")
+        with open(tmp, "wb") as f:
+            pickle.dump((key, compiled), f, protocol=pickle.HIGHEST_PROTOCOL)
+        os.replace(tmp, path)
+    except Exception:
+        pass
 
 
 def runtime_const_values(compiled, runtime_consts, const_values, use_defaults):

@@ -1,0 +1,381 @@
+"""Continuous-batching sweep server.
+
+Requests - any ``mesolve_2D`` / ``odesolve_2D`` call, of any model, size, integrator or form - are
+admitted while device memory and slots allow, split into point chunks, and their chunks are
+interleaved across several CUDA streams, so work of requests that arrive while others run overlaps
+on the device. Inputs and outputs stay resident in device memory from admission to completion;
+adaptive requests keep work stealing inside each chunk. The server loop is one host thread; every
+launch goes through the model module's C ABI (``gqis_sweep_launch``), a chunk being the descriptor's
+``[point_begin, point_begin + point_count)`` slice with per-point pointers offset to that slice.
+
+Each point's result depends only on its own inputs, so a request returns the same values alone and
+in the mix (the GPU tests check that bit for bit).
+
+The device layer is a small backend object so that the scheduling logic (admission by memory
+budget and slots, round-robin dispatch, cancellation, failure isolation) is tested on the CPU with
+a fake backend.
+"""
+
+from __future__ import annotations
+
+import itertools
+import threading
+import time
+from collections import deque
+from dataclasses import dataclass, field
+
+import numpy as np
+
+QUEUED, RUNNING, DONE, FAILED, CANCELLED = "queued", "running", "done", "failed", "cancelled"
+
+
+class SweepFuture:
+    """Handle of one submitted request."""
+
+    def __init__(self, rid, arrival):
+        self.id = rid
+        self.arrival = arrival
+        self.admitted_at = None
+        self.finished_at = None
+        self.state = QUEUED
+        self.error = None
+        self._result = None
+        self._event = threading.Event()
+
+    def done(self):
+        return self._event.is_set()
+
+    def result(self, timeout=None):
+        if not self._event.wait(timeout):
+            raise TimeoutError(f"request {self.id} not finished within {timeout} s")
+        if self.state == FAILED:
+            raise RuntimeError(f"request {self.id} failed: {self.error}")
+        if self.state == CANCELLED:
+            raise RuntimeError(f"request {self.id} was cancelled")
+        return self._result
+
+    @property
+    def latency(self):
+        return None if self.finished_at is None else self.finished_at - self.arrival
+
+    def _finish(self, state, result=None, error=None):
+        self.state, self._result, self.error = state, result, error
+        self.finished_at = time.perf_counter()
+        self._event.set()
+
+
+@dataclass
+class _Request:
+    future: SweepFuture
+    launch: object                 # solver.SweepLaunch (or a backend-specific description)
+    shape: tuple                   # output post-processing information
+    nbytes: int
+    points: int
+    point_steps: int
+    chunks: deque = field(default_factory=deque)
+    inflight: list = field(default_factory=list)
+    handle: object = None          # backend state (device buffers)
+    cancel: bool = False
+    copying: object = None
+
+
+class TorchBackend:
+    """Device layer on torch tensors and CUDA streams; launches through the model modules' C ABI."""
+
+    def __init__(self, device=0, streams=4):
+        import torch
+        self.torch = torch
+        self.device = torch.device("cuda", device)
+        with torch.cuda.device(self.device):
+            self.admit_stream = torch.cuda.Stream(self.device)
+            self.streams = [torch.cuda.Stream(self.device) for _ in range(streams)]
+
+    def free_bytes(self):
+        free, _total = self.torch.cuda.mem_get_info(self.device)
+        return free
+
+    def admit(self, req, chunk_points):
+        """Allocate and upload on the admission stream; returns the chunk list."""
+        from . import abi, solver
+        torch = self.torch
+        with torch.cuda.device(self.device), torch.cuda.stream(self.admit_stream):
+            module = solver._load_kernel(req.launch.entry)
+            desc, buf = solver._device_buffers(req.launch)
+            n = int(desc.point_count)
+            starts = list(range(0, n, chunk_points))
+            counters = (torch.zeros(len(starts), dtype=torch.int32, device=self.device)
+                        if req.launch.adaptive else None)
+            ready = torch.cuda.Event()
+            ready.record(self.admit_stream)
+        real = buf["results"].element_size()
+        width = buf["results"].shape[1]
+        chunks = []
+        for k, b in enumerate(starts):
+            c = abi.SweepDesc.from_buffer_copy(desc)
+            c.point_begin, c.point_count = b, min(chunk_points, n - b)
+            c.results = desc.results + b * width * real
+            if desc.rho0:
+                c.rho0 = desc.rho0 + b * buf["rho0"].shape[1] * real
+            if desc.trace:
+                tr = buf["trace"]
+                c.trace = desc.trace + b * tr.shape[1] * tr.shape[2] * real
+            if desc.step_counts:
+                c.step_counts = desc.step_counts + b * 2 * 4
+            if counters is not None:
+                c.work_counter = counters.data_ptr() + 4 * k
+            chunks.append(c)
+        req.handle = {"module": module, "buf": buf, "desc": desc, "ready": ready, "counters": counters}
+        return chunks
+
+    def launch(self, req, chunk, stream_index):
+        torch = self.torch
+        st = self.streams[stream_index]
+        st.wait_event(req.handle["ready"])
+        req.handle["module"].launch(chunk, st.cuda_stream)
+        ev = torch.cuda.Event()
+        ev.record(st)
+        return ev
+
+    @staticmethod
+    def query(event):
+        return event.query()
+
+    def copy_out(self, req, events):
+        """D2H of the results after the given chunk events; returns an event."""
+        torch = self.torch
+        with torch.cuda.device(self.device), torch.cuda.stream(self.admit_stream):
+            for ev in events:
+                self.admit_stream.wait_event(ev)
+            host = {}
+            for name in ("results", "trace", "step_counts"):
+                t = req.handle["buf"][name]
+                if t is not None:
+                    h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+                    h.copy_(t, non_blocking=True)
+                    host[name] = h
+            ev = torch.cuda.Event()
+            ev.record(self.admit_stream)
+        req.handle["host"] = host
+        return ev
+
+    def results(self, req):
+        return {k: v.numpy() for k, v in req.handle["host"].items()}
+
+    def release(self, req):
+        req.handle = None
+
+
+class SweepServer:
+    """Continuous-batching server (see the module docstring).
+
+    ``memory_budget`` caps the device bytes of admitted requests (default: half the free memory at
+    start); ``max_inflight`` caps admitted requests; ``chunk_points`` is the launch granularity.
+    """
+
+    def __init__(self, device=0, streams=4, memory_budget=None, max_inflight=16, chunk_points=1 << 16,
+                 backend=None, poll_s=50e-6):
+        self.backend = backend or TorchBackend(device, streams)
+        self.nstreams = len(getattr(self.backend, "streams", [None] * streams))
+        self.budget = int(memory_budget if memory_budget is not None else self.backend.free_bytes() // 2)
+        self.max_inflight = int(max_inflight)
+        self.chunk_points = int(chunk_points)
+        self.poll_s = poll_s
+        self._ids = itertools.count()
+        self._lock = threading.Lock()
+        self._queue = deque()
+        self._active = []
+        self._used = 0
+        self._stop = False
+        self._stream_load = [0] * self.nstreams
+        self.stats = {"submitted": 0, "completed": 0, "failed": 0, "cancelled": 0, "point_steps": 0,
+                      "max_concurrent": 0}
+        self._thread = threading.Thread(target=self._loop, name="gqis-serve", daemon=True)
+        self._thread.start()
+
+    # ------------------------------------------------------------------ public API
+    def submit(self, api, *args, **kwargs):
+        """Queue one ``mesolve_2D`` / ``odesolve_2D`` call; returns a :class:`SweepFuture`.
+
+        The symbolic preparation and the module build run here, in the caller's thread (both are
+        cached), so the server thread only moves data and launches kernels.
+        """
+        from . import solver
+        holder = {}
+        kwargs = dict(kwargs, _prepare_only=holder)
+        if api in ("odesolve_2D", "odesolve"):
+            from .gqis_ode_api import odesolve_2D
+            odesolve_2D(*args, **kwargs)
+        else:
+            solver.mesolve_2D(*args, **kwargs)
+        launch = holder["launch"]
+        solver._load_kernel(launch.entry)
+        return self.submit_launch(launch)
+
+    def submit_launch(self, launch, nbytes=None):
+        rid = next(self._ids)
+        fut = SweepFuture(rid, time.perf_counter())
+        nx = len(launch.par_x)
+        ny = len(launch.par_y)
+        points = nx * ny
+        if nbytes is None:
+            real = 8 if launch.form == "fp64" else 4
+            width = 2 if launch.output_mode in ("mean", "final") else launch.state_size
+            nbytes = points * width * real + 8 * (nx + ny + len(launch.consts) + 1)
+            if launch.rho0 is not None:
+                nbytes += points * launch.state_size * real
+            if launch.trace_mode is not None:
+                tw = 2 if launch.trace_mode == "observable" else launch.state_size
+                nbytes += points * launch.num_trace * tw * real
+        req = _Request(fut, launch, (nx, ny), int(nbytes), points, points * int(launch.num_steps))
+        if req.nbytes > self.budget:
+            fut._finish(FAILED, error=f"request needs {req.nbytes} bytes, more than the budget {self.budget}")
+            return fut
+        with self._lock:
+            self._queue.append(req)
+            self.stats["submitted"] += 1
+        return fut
+
+    def cancel(self, fut):
+        with self._lock:
+            for req in list(self._queue):
+                if req.future is fut:
+                    self._queue.remove(req)
+                    fut._finish(CANCELLED)
+                    self.stats["cancelled"] += 1
+                    return True
+            for req in self._active:
+                if req.future is fut:
+                    req.cancel = True
+                    return True
+        return False
+
+    def close(self, timeout=60.0):
+        self._stop = True
+        self._thread.join(timeout)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ------------------------------------------------------------------ server loop
+    def _admit(self):
+        while True:
+            with self._lock:
+                if not self._queue or len(self._active) >= self.max_inflight:
+                    return
+                req = self._queue[0]
+                if self._used + req.nbytes > self.budget:
+                    return
+                self._queue.popleft()
+            try:
+                req.chunks = deque(self.backend.admit(req, self.chunk_points))
+            except Exception as exc:  # allocation or upload failure: this request only
+                req.future._finish(FAILED, error=repr(exc))
+                self.stats["failed"] += 1
+                continue
+            req.future.state = RUNNING
+            req.future.admitted_at = time.perf_counter()
+            self._used += req.nbytes
+            with self._lock:
+                self._active.append(req)
+                self.stats["max_concurrent"] = max(self.stats["max_concurrent"], len(self._active))
+
+    def _dispatch(self):
+        # Round-robin over admitted requests: one chunk each per pass, onto the least-loaded
+        # stream, at most two chunks queued per stream.
+        progressed = False
+        for req in list(self._active):
+            if req.cancel or not req.chunks or req.copying is not None:
+                continue
+            s = min(range(self.nstreams), key=lambda i: self._stream_load[i])
+            if self._stream_load[s] >= 2:
+                break
+            chunk = req.chunks.popleft()
+            try:
+                ev = self.backend.launch(req, chunk, s)
+            except Exception as exc:
+                req.cancel = True
+                req.future.error = repr(exc)
+                continue
+            self._stream_load[s] += 1
+            req.inflight.append((ev, s))
+            progressed = True
+        return progressed
+
+    def _complete(self):
+        progressed = False
+        for req in list(self._active):
+            still = []
+            for ev, s in req.inflight:
+                if self.backend.query(ev):
+                    self._stream_load[s] -= 1
+                    progressed = True
+                else:
+                    still.append((ev, s))
+            req.inflight = still
+            if req.inflight:
+                continue
+            if req.cancel:
+                state = FAILED if req.future.error else CANCELLED
+                self._retire(req, state, error=req.future.error)
+                progressed = True
+            elif not req.chunks:
+                if req.copying is None:
+                    req.copying = self.backend.copy_out(req, [])
+                elif self.backend.query(req.copying):
+                    out = self.backend.results(req)
+                    self._retire(req, DONE, result=out)
+                    progressed = True
+        return progressed
+
+    def _retire(self, req, state, result=None, error=None):
+        self.backend.release(req)
+        self._used -= req.nbytes
+        with self._lock:
+            self._active.remove(req)
+        if state == DONE:
+            self.stats["completed"] += 1
+            self.stats["point_steps"] += req.point_steps
+            result = _shape_outputs(req, result)
+        elif state == FAILED:
+            self.stats["failed"] += 1
+        else:
+            self.stats["cancelled"] += 1
+        req.future._finish(state, result=result, error=error)
+
+    def _loop(self):
+        while True:
+            self._admit()
+            busy = self._dispatch()
+            busy = self._complete() or busy
+            with self._lock:
+                idle = not self._active and not self._queue
+            if self._stop and idle:
+                return
+            if not busy:
+                time.sleep(self.poll_s)
+
+
+def _shape_outputs(req, out):
+    """Server outputs -> the shapes ``mesolve_2D`` returns (complex maps, state arrays, traces)."""
+    launch = req.launch
+    nx, ny = req.shape
+    res = np.asarray(out["results"])
+    if launch.output_mode in ("mean", "final"):
+        r = res.reshape(nx, ny, 2)
+        result = r[..., 0] + 1j * r[..., 1]
+    else:
+        result = res.reshape(nx, ny, launch.state_size)
+    payload = {"result": result}
+    if out.get("trace") is not None:
+        tr = np.asarray(out["trace"])
+        if launch.trace_mode == "observable":
+            tr = tr.reshape(nx, ny, launch.num_trace, 2)
+            payload["trace"] = tr[..., 0] + 1j * tr[..., 1]
+        else:
+            payload["trace"] = tr.reshape(nx, ny, launch.num_trace, launch.state_size)
+    if out.get("step_counts") is not None:
+        payload["step_counts"] = np.asarray(out["step_counts"]).reshape(nx, ny, 2)
+    return payload

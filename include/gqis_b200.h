@@ -141,6 +141,32 @@ const char* gqis_last_error(void);
 #define GQIS_NOALLOC_MAX_POINTS 2147483647LL
 int gqis_sweep_launch_noalloc(const gqis_sweep_desc* desc, void* stream);
 
+/* ---------------------------------------------------------------------------------------
+ * Gradients (adjoint modules). No counterpart in the reference, which has no derivatives: a
+ * module built with an adjoint (gqis.adjoint) also exports the functions below. For every point
+ * they return <O>_avg (the RK4 right-endpoint time average, FP64, bit-identical to the sweep's
+ * mean output) and its exact derivative with respect to the module's P parameters (runtime
+ * constants and/or sweep parameters), by the discrete adjoint of the RK4 steps with checkpoints.
+ * --------------------------------------------------------------------------------------- */
+typedef struct gqis_adjoint_desc {
+    gqis_sweep_desc sweep;          /* grid, steps, warmup, dt, t_in, inputs; results = [points, 2] FP64 */
+    int32_t num_params;             /* P; must equal the module's */
+    int32_t checkpoint_every;       /* steps between stored states (ceil(sqrt(num_steps)) balances memory and time) */
+    const double* adjoint_consts;   /* full runtime-constant array in the adjoint's order, or NULL */
+    double* grad;                   /* [point_count, P] d<O>_avg / dtheta */
+    double* scratch;                /* gqis_adjoint_scratch_bytes() bytes of device memory (checkpoints) */
+    int64_t scratch_bytes;
+} gqis_adjoint_desc;
+
+/* Parameters and state size of the module's adjoint (GQIS_ERR_UNSUPPORTED if it has none). */
+int gqis_adjoint_info(int32_t* num_params, int32_t* state_size);
+
+/* Device scratch needed by gqis_adjoint_launch for this many points, steps and checkpoint interval. */
+int gqis_adjoint_scratch_bytes(int64_t point_count, int32_t num_steps, int32_t checkpoint_every, int64_t* bytes);
+
+/* Mean map and its parameter gradient; asynchronous on stream. */
+int gqis_adjoint_launch(const gqis_adjoint_desc* desc, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

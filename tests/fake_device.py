@@ -53,7 +53,8 @@ def clear_caches():
 def fake_device(values=None):
     dev = FakeDevice(values)
     clear_caches()
-    with patch.object(core, "_load_kernel", dev.load_kernel), patch.object(core, "_device_run", dev.device_run):
+    with patch.dict("os.environ", {"GQIS_DISK_CACHE": "0"}), \
+            patch.object(core, "_load_kernel", dev.load_kernel), patch.object(core, "_device_run", dev.device_run):
         try:
             yield dev
         finally:

@@ -1,0 +1,55 @@
+"""The continuous-batching server on the GPU: every result is the same alone and in the mix."""
+
+import numpy as np
+import pytest
+
+import ref_cases
+
+
+def _direct(case):
+    import gqis
+    return getattr(gqis, case["api"])(*case["args"], **case["kwargs"])
+
+
+@pytest.mark.gpu
+def test_each_request_is_the_same_alone_and_in_the_mix():
+    from gqis.serving import SweepServer
+    cases = ref_cases.cases()
+    names = ["c1_fp64_mean", "c2_fp64_mean_sub32", "qubit_dop853_final_rho", "qubit_rk4_mean_warmup_trace",
+             "qubit_tsit5a_mean", "duffing_tsit5a_trace", "duffing_rk4_observable_trace", "qubit_ab5_final_rho"]
+    alone = {n: _direct(cases[n]) for n in names}
+    # Small chunks and several streams: the requests' chunks interleave and overlap on the device.
+    with SweepServer(streams=3, chunk_points=256, max_inflight=8) as srv:
+        futs = {n: srv.submit(cases[n]["api"], *cases[n]["args"], **cases[n]["kwargs"]) for n in names}
+        outs = {n: f.result(300) for n, f in futs.items()}
+        stats = dict(srv.stats)
+    assert stats["completed"] == len(names)
+    assert stats["max_concurrent"] >= 2
+    for n in names:
+        ref = alone[n]
+        ref_result = ref[0] if isinstance(ref, tuple) else ref
+        np.testing.assert_array_equal(outs[n]["result"], ref_result, err_msg=n)
+        if isinstance(ref, tuple):
+            np.testing.assert_array_equal(outs[n]["trace"], ref[1], err_msg=n)
+
+
+@pytest.mark.gpu
+def test_server_isolates_a_request_the_c_abi_rejects():
+    """A launch the module rejects (status != 0) fails its own request; the others complete."""
+    import dataclasses
+    import gqis
+    from gqis import solver
+    from gqis.serving import FAILED, SweepServer
+    good = ref_cases.cases()["qubit_rk4_final"]
+    holder = {}
+    gqis.mesolve_2D(*good["args"], **good["kwargs"], _prepare_only=holder)
+    solver._load_kernel(holder["launch"].entry)
+    bad = dataclasses.replace(holder["launch"], num_steps=0)  # "num_steps must be at least 1"
+    with SweepServer(streams=2, chunk_points=16) as srv:
+        f1 = srv.submit(good["api"], *good["args"], **good["kwargs"])
+        f2 = srv.submit_launch(bad)
+        f3 = srv.submit(good["api"], *good["args"], **good["kwargs"])
+        r1, r3 = f1.result(120), f3.result(120)
+        f2._event.wait(120)
+    np.testing.assert_array_equal(r1["result"], r3["result"])
+    assert f2.state == FAILED and "num_steps" in f2.error
