@@ -37,7 +37,14 @@ class SweepDesc(ctypes.Structure):
                 ("solver_params", ctypes.c_double * 8)]
 
 
-MODULE_SYMBOLS = ("gqis_model_info_get", "gqis_sweep_launch", "gqis_last_error", "gqis_sweep_launch_noalloc")
+class AdjointDesc(ctypes.Structure):
+    _fields_ = [("sweep", SweepDesc), ("num_params", ctypes.c_int32), ("checkpoint_every", ctypes.c_int32),
+                ("adjoint_consts", ctypes.c_void_p), ("grad", ctypes.c_void_p), ("scratch", ctypes.c_void_p),
+                ("scratch_bytes", ctypes.c_int64)]
+
+
+MODULE_SYMBOLS = ("gqis_model_info_get", "gqis_sweep_launch", "gqis_last_error", "gqis_sweep_launch_noalloc",
+                  "gqis_adjoint_info", "gqis_adjoint_scratch_bytes", "gqis_adjoint_launch")
 
 
 def bind_module(lib):
@@ -48,6 +55,13 @@ def bind_module(lib):
     lib.gqis_sweep_launch.restype = ctypes.c_int
     lib.gqis_sweep_launch_noalloc.argtypes = [ctypes.POINTER(SweepDesc), ctypes.c_void_p]
     lib.gqis_sweep_launch_noalloc.restype = ctypes.c_int
+    lib.gqis_adjoint_info.argtypes = [ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]
+    lib.gqis_adjoint_info.restype = ctypes.c_int
+    lib.gqis_adjoint_scratch_bytes.argtypes = [ctypes.c_int64, ctypes.c_int32, ctypes.c_int32,
+                                               ctypes.POINTER(ctypes.c_int64)]
+    lib.gqis_adjoint_scratch_bytes.restype = ctypes.c_int
+    lib.gqis_adjoint_launch.argtypes = [ctypes.POINTER(AdjointDesc), ctypes.c_void_p]
+    lib.gqis_adjoint_launch.restype = ctypes.c_int
     lib.gqis_last_error.argtypes = []
     lib.gqis_last_error.restype = ctypes.c_char_p
 

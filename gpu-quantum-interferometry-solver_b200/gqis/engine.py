@@ -77,8 +77,8 @@ def templates_digest() -> str:
     return _TEMPLATE_DIGEST
 
 
-def module_source(frag, spec, form, output_mode, trace_mode, unroll=False):
-    """Complete translation unit of one model variant."""
+def module_source(frag, spec, form, output_mode, trace_mode, unroll=False, extra_code="", defines=None):
+    """Complete translation unit of one model variant (``extra_code`` goes into ``gqmodel``)."""
     model = emit.model_source(frag)
     model_hash = int(hashlib.sha256(model.encode()).hexdigest()[:16], 16)
     lines = [
@@ -87,6 +87,7 @@ def module_source(frag, spec, form, output_mode, trace_mode, unroll=False):
         "namespace gqmodel {",
         model,
         tableau_source(spec),
+        extra_code,
         "}  // namespace gqmodel",
         "#define GQ_MODEL gqmodel::Model",
         f"#define GQ_FORM {FORM_TYPES[form]}",
@@ -96,6 +97,7 @@ def module_source(frag, spec, form, output_mode, trace_mode, unroll=False):
         f"#define GQ_OUT {OUTPUT_MODES[output_mode]}",
         f"#define GQ_TRACE {TRACE_MODES[trace_mode]}",
         f"#define GQ_MODEL_HASH 0x{model_hash:016x}ULL",
+        *[f"#define {k} {v}" for k, v in (defines or {}).items()],
         '#include "gqis_module.cuh"',
         "",
     ]

@@ -65,6 +65,23 @@ class SweepFuture:
 
 
 @dataclass
+class FitLaunch:
+    """A gradient ("fit") request: the adjoint module and the sweep it differentiates."""
+
+    sweep: object          # solver.SweepLaunch of the mean map
+    module: object         # adjoint module (engine.ModelModule)
+    P: int
+    params: list
+    checkpoint_every: int
+    forward_consts: list
+    adjoint_consts: list
+
+    # the attributes the server reads for budgeting and output shapes
+    def __getattr__(self, name):
+        return getattr(self.sweep, name)
+
+
+@dataclass
 class _Request:
     future: SweepFuture
     launch: object                 # solver.SweepLaunch (or a backend-specific description)
@@ -77,6 +94,7 @@ class _Request:
     handle: object = None          # backend state (device buffers)
     cancel: bool = False
     copying: object = None
+    kind: str = "sweep"
 
 
 class TorchBackend:
@@ -96,6 +114,8 @@ class TorchBackend:
 
     def admit(self, req, chunk_points):
         """Allocate and upload on the admission stream; returns the chunk list."""
+        if req.kind == "adjoint":
+            return self._admit_adjoint(req, chunk_points)
         from . import abi, solver
         torch = self.torch
         with torch.cuda.device(self.device), torch.cuda.stream(self.admit_stream):
@@ -127,11 +147,58 @@ class TorchBackend:
         req.handle = {"module": module, "buf": buf, "desc": desc, "ready": ready, "counters": counters}
         return chunks
 
+    def _admit_adjoint(self, req, chunk_points):
+        import ctypes
+        from . import abi, solver
+        torch = self.torch
+        fit = req.launch  # FitLaunch
+        with torch.cuda.device(self.device), torch.cuda.stream(self.admit_stream):
+            desc, buf = solver._device_buffers(fit.sweep)
+            n = int(desc.point_count)
+            N = int(fit.sweep.num_steps)
+            region = ctypes.c_int64()
+            rc = fit.module.lib.gqis_adjoint_scratch_bytes(min(chunk_points, n), N, fit.checkpoint_every,
+                                                           ctypes.byref(region))
+            abi.check(rc, fit.module.lib)
+            starts = list(range(0, n, chunk_points))
+            words = (region.value + 7) // 8
+            scratch = torch.empty(max(1, words * len(starts)), dtype=torch.float64, device=self.device)
+            grad = torch.empty((n, max(1, fit.P)), dtype=torch.float64, device=self.device)
+            cf = torch.tensor(fit.forward_consts or [0.0], dtype=torch.float64, device=self.device)
+            ca = torch.tensor(fit.adjoint_consts or [0.0], dtype=torch.float64, device=self.device)
+            ready = torch.cuda.Event()
+            ready.record(self.admit_stream)
+        buf["grad"] = grad
+        chunks = []
+        for k, b in enumerate(starts):
+            a = abi.AdjointDesc()
+            a.sweep = abi.SweepDesc.from_buffer_copy(desc)
+            a.sweep.point_begin, a.sweep.point_count = b, min(chunk_points, n - b)
+            a.sweep.results = desc.results + b * 2 * 8
+            a.sweep.consts = cf.data_ptr() if fit.forward_consts else None
+            a.num_params = fit.P
+            a.checkpoint_every = fit.checkpoint_every
+            a.adjoint_consts = ca.data_ptr()
+            a.grad = grad.data_ptr() + b * max(1, fit.P) * 8
+            a.scratch = scratch.data_ptr() + k * words * 8
+            a.scratch_bytes = words * 8
+            chunks.append(a)
+        req.handle = {"module": fit.module, "buf": buf, "desc": desc, "ready": ready,
+                      "keep": (scratch, cf, ca)}
+        return chunks
+
     def launch(self, req, chunk, stream_index):
         torch = self.torch
         st = self.streams[stream_index]
         st.wait_event(req.handle["ready"])
-        req.handle["module"].launch(chunk, st.cuda_stream)
+        if req.kind == "adjoint":
+            import ctypes
+            from . import abi
+            lib = req.handle["module"].lib
+            rc = lib.gqis_adjoint_launch(ctypes.byref(chunk), ctypes.c_void_p(st.cuda_stream))
+            abi.check(rc, lib)
+        else:
+            req.handle["module"].launch(chunk, st.cuda_stream)
         ev = torch.cuda.Event()
         ev.record(st)
         return ev
@@ -147,8 +214,8 @@ class TorchBackend:
             for ev in events:
                 self.admit_stream.wait_event(ev)
             host = {}
-            for name in ("results", "trace", "step_counts"):
-                t = req.handle["buf"][name]
+            for name in ("results", "trace", "step_counts", "grad"):
+                t = req.handle["buf"].get(name)
                 if t is not None:
                     h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
                     h.copy_(t, non_blocking=True)
@@ -211,7 +278,27 @@ class SweepServer:
         solver._load_kernel(launch.entry)
         return self.submit_launch(launch)
 
-    def submit_launch(self, launch, nbytes=None):
+    def submit_fit(self, *args, params, values=None, checkpoint_every=None, **kwargs):
+        """Queue a gradient request: the ``mesolve_2D`` mean map and d<O>_avg/dtheta per point for the
+        runtime-constant parameters ``params`` (checkpointed RK4 adjoint, FP64)."""
+        import math
+        from . import adjoint, engine
+        source, launch, meta = adjoint.module_source(*args, params=params, **kwargs)
+        module = engine.load_module(source)
+        prob_consts = adjoint.const_values(launch.entry["compiled"], meta["defaults"], values)
+        used = launch.entry["frag"]["used_const_indices"]
+        fit = FitLaunch(sweep=launch, module=module, P=meta["P"], params=meta["params"],
+                        checkpoint_every=int(checkpoint_every or max(1, math.ceil(math.sqrt(launch.num_steps)))),
+                        forward_consts=[prob_consts[i] for i in used] if used else [],
+                        adjoint_consts=prob_consts)
+        points = len(launch.par_x) * len(launch.par_y)
+        ck = fit.checkpoint_every
+        scratch = (math.ceil(launch.num_steps / ck) + ck) * launch.state_size * min(points, self.chunk_points) * 8
+        nchunks = math.ceil(points / self.chunk_points)
+        nbytes = points * (2 + fit.P) * 8 + scratch * nchunks
+        return self.submit_launch(fit, nbytes=nbytes, kind="adjoint")
+
+    def submit_launch(self, launch, nbytes=None, kind="sweep"):
         rid = next(self._ids)
         fut = SweepFuture(rid, time.perf_counter())
         nx = len(launch.par_x)
@@ -226,7 +313,7 @@ class SweepServer:
             if launch.trace_mode is not None:
                 tw = 2 if launch.trace_mode == "observable" else launch.state_size
                 nbytes += points * launch.num_trace * tw * real
-        req = _Request(fut, launch, (nx, ny), int(nbytes), points, points * int(launch.num_steps))
+        req = _Request(fut, launch, (nx, ny), int(nbytes), points, points * int(launch.num_steps), kind=kind)
         if req.nbytes > self.budget:
             fut._finish(FAILED, error=f"request needs {req.nbytes} bytes, more than the budget {self.budget}")
             return fut
@@ -378,4 +465,9 @@ def _shape_outputs(req, out):
             payload["trace"] = tr.reshape(nx, ny, launch.num_trace, launch.state_size)
     if out.get("step_counts") is not None:
         payload["step_counts"] = np.asarray(out["step_counts"]).reshape(nx, ny, 2)
+    if out.get("grad") is not None:
+        P = launch.P
+        payload["result"] = payload["result"].real
+        payload["grad"] = np.asarray(out["grad"])[:, :P].reshape(nx, ny, P)
+        payload["params"] = launch.params
     return payload

@@ -555,7 +555,7 @@ def _solve_symbolic_system(H, Drive, Col_Ops, mean_operator, tlist,
         from . import engine
         entry = {"source": engine.module_source(frag, spec, form, mode, trace_mode, unroll),
                  "module": None, "flags": flags + (("-DGQ_FULL_UNROLL=1",) if unroll else ()),
-                 "frag": frag, "spec": spec}
+                 "frag": frag, "spec": spec, "compiled": compiled}
         if RHSreuse:
             _KERNEL_CACHE[kkey] = entry
     else:

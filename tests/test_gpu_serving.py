@@ -53,3 +53,20 @@ def test_server_isolates_a_request_the_c_abi_rejects():
         f2._event.wait(120)
     np.testing.assert_array_equal(r1["result"], r3["result"])
     assert f2.state == FAILED and "num_steps" in f2.error
+
+
+@pytest.mark.gpu
+def test_fit_requests_in_the_server_match_the_adjoint_alone():
+    from gqis import adjoint
+    from gqis.serving import SweepServer
+    from test_support_calls import qubit_fit_model
+    args, kwargs, params = qubit_fit_model()
+    mean, grad = adjoint.mean_gradient(*args, **kwargs, params=list(params[:3]))
+    sweep_case = ref_cases.cases()["c1_fp64_mean"]
+    with SweepServer(streams=2, chunk_points=16) as srv:
+        f_fit = srv.submit_fit(*args, **kwargs, params=list(params[:3]))
+        f_sweep = srv.submit(sweep_case["api"], *sweep_case["args"], **sweep_case["kwargs"])
+        out = f_fit.result(300)
+        f_sweep.result(300)
+    np.testing.assert_array_equal(out["result"], mean)
+    np.testing.assert_array_equal(out["grad"], grad)

@@ -49,3 +49,25 @@ def calls():
             _, args, kwargs = duffing_case(solver=solver, **extra)
             out.append(("odesolve_2D", args, kwargs))
     return out
+
+
+def qubit_fit_model(side=(8, 6), steps=400, duration=20.0):
+    """Two-level model with Gamma1, Gamma_phi and Delta kept symbolic (fit parameters)."""
+    import sympy as sp
+    eps, A, D, Drive, t, G1, Gp = sp.symbols("eps A Delta Drive t Gamma1 Gammaphi", real=True)
+    sz, sx, sm = sp.Matrix([[1, 0], [0, -1]]), sp.Matrix([[0, 1], [1, 0]]), sp.Matrix([[0, 1], [0, 0]])
+    H = eps / 2 * sz + D / 2 * sx + Drive * sz
+    args = (H, A * sp.cos(sp.pi * t), [sp.sqrt(G1) * sm, sp.sqrt(Gp / 2) * sz], sp.diag(0, 1),
+            np.linspace(0.0, duration, steps + 1))
+    kwargs = {"var_arrays": {eps: np.linspace(-3.0, 3.0, side[0]), A: np.linspace(0.0, 2.0, side[1])},
+              "runtime_consts": {G1: 0.01, Gp: 0.02, D: 1.0}}
+    return args, kwargs, (G1, Gp, D, A)
+
+
+def adjoint_problems():
+    """(args, kwargs) of the adjoint problems the GPU tests and the serving bench build."""
+    args, kwargs, params = qubit_fit_model()
+    out = [(args, dict(kwargs, params=list(params))), (args, dict(kwargs, params=list(params[:3])))]
+    args, kwargs, params = qubit_fit_model(side=(256, 256), steps=4000, duration=200.0)
+    out.append((args, dict(kwargs, params=list(params[:3]))))
+    return out
