@@ -393,26 +393,34 @@ def run_serving(args):
     sys.path.insert(0, str(ROOT / "tests"))
     sys.path.insert(0, str(ROOT / "oracle"))
     import gqis
+    from gqis import adjoint
     from gqis.serving import SweepServer
-    from test_support_calls import SERVING_SIDES, serving_model
+    from test_support_calls import SERVING_SIDES, qubit_fit_model, serving_model
     rng = np.random.default_rng(args.seed)
     dims = (2, 4, 8)
     reqs = []
     t = 0.0
     for _ in range(args.requests):
         t += rng.exponential(1.0 / args.rate)
-        N = int(rng.choice(dims))
-        side = int(rng.choice(SERVING_SIDES))
-        reqs.append((t, N, side))
+        if rng.random() < 0.2:
+            reqs.append((t, "fit", 256))
+        else:
+            reqs.append((t, int(rng.choice(dims)), int(rng.choice(SERVING_SIDES))))
     models = {}
     for _, N, side in reqs:
-        if (N, side) not in models:
+        if N != "fit" and (N, side) not in models:
             models[(N, side)] = serving_model(N, side)
+    fit_args, fit_kwargs, fit_params = qubit_fit_model(side=(256, 256), steps=4000, duration=200.0)
+    fit_params = list(fit_params[:3])
     for N in dims:  # warm the caches (symbolic model, module load) before timing
         a, kw = serving_model(N, 64)
         gqis.mesolve_2D(*a, **kw, precision="fp32")
         gqis.mesolve_2D(*a, **kw, precision="fp64")
-    point_steps = sum(side * side * (len(models[(N, side)][0][4]) - 1) for _, N, side in reqs)
+    adjoint.module_source(*fit_args, **fit_kwargs, params=fit_params)
+
+    def steps_of(N, side):
+        return 4000 if N == "fit" else len(models[(N, side)][0][4]) - 1
+    point_steps = sum(side * side * steps_of(N, side) for _, N, side in reqs)
     futs = []
     with SweepServer(streams=4, chunk_points=1 << 15, max_inflight=16) as srv:
         t0 = time.perf_counter()
@@ -420,10 +428,12 @@ def run_serving(args):
             delay = t0 + arrival - time.perf_counter()
             if delay > 0:
                 time.sleep(delay)
-            a, kw = models[(N, side)]
-            futs.append(srv.submit("mesolve_2D", *a, **kw, precision="fp32"))
-        for f in futs:
-            f.result(600)
+            if N == "fit":
+                futs.append(srv.submit_fit(*fit_args, **fit_kwargs, params=fit_params))
+            else:
+                a, kw = models[(N, side)]
+                futs.append(srv.submit("mesolve_2D", *a, **kw, precision="fp32"))
+        outs = [f.result(900) for f in futs]
         t_end = max(f.finished_at for f in futs)
         stats = dict(srv.stats)
     lat = np.array([f.latency for f in futs]) * 1e3
@@ -431,22 +441,46 @@ def run_serving(args):
     torch.cuda.synchronize()
     t1 = time.perf_counter()
     for _, N, side in reqs:  # the same requests one by one on the plain FP64 path
-        a, kw = models[(N, side)]
-        gqis.mesolve_2D(*a, **kw, precision="fp64")
+        if N == "fit":
+            adjoint.mean_gradient(*fit_args, **fit_kwargs, params=fit_params)
+        else:
+            a, kw = models[(N, side)]
+            gqis.mesolve_2D(*a, **kw, precision="fp64")
     torch.cuda.synchronize()
     seq = point_steps / (time.perf_counter() - t1)
+    # one fit result against central differences (h = 1e-6, FP64) on a 16 x 16 strided subgrid
+    fit_check = None
+    fit_idx = [k for k, (_, N, _) in enumerate(reqs) if N == "fit"]
+    if fit_idx:
+        grad = outs[fit_idx[0]]["grad"]
+        sel = np.round(np.linspace(0, 255, 16)).astype(int)
+        (es, As) = list(fit_kwargs["var_arrays"])
+        sub = dict(fit_kwargs, var_arrays={es: fit_kwargs["var_arrays"][es][sel], As: fit_kwargs["var_arrays"][As][sel]})
+        errs = []
+        for m, p in enumerate(fit_params):
+            up, dn = dict(sub["runtime_consts"]), dict(sub["runtime_consts"])
+            up[p] += 1e-6
+            dn[p] -= 1e-6
+            fd = (gqis.mesolve_2D(*fit_args, **dict(sub, runtime_consts=up), fp64=True).real
+                  - gqis.mesolve_2D(*fit_args, **dict(sub, runtime_consts=dn), fp64=True).real) / 2e-6
+            g = grad[np.ix_(sel, sel)][..., m]
+            errs.append(float(np.max(np.abs(g - fd)) / np.max(np.abs(fd))))
+        fit_check = {"params": [str(p) for p in fit_params], "max_rel_err_vs_central_fd": errs}
     line = {
-        "metric": "sweep serving: aggregate points*steps/s and latency (Poisson 50/s, N in {2,4,8})",
+        "metric": "sweep serving: aggregate points*steps/s and latency (Poisson 50/s, N in {2,4,8}, 20% fits)",
         "value": served, "unit": "points*steps/s", "n_gpus": 1, "steps": args.requests, "warmup": len(dims),
         "ms_per_step": float(np.mean(lat)), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"{args.requests} seeded requests, Poisson rate {args.rate}/s, N uniform in {dims}, "
-                               f"grid side uniform in {SERVING_SIDES}, mean <O> maps, RK4 (model tlists)",
+        "config": {"workload": f"{args.requests} seeded requests, Poisson rate {args.rate}/s; 80% sweeps (N uniform "
+                               f"in {dims}, grid side uniform in {SERVING_SIDES}, mean <O> maps, RK4, FP32 form), "
+                               "20% fits (d<O>avg/d(Gamma1, Gamma_phi, Delta), 256x256 two-level map, 4000 RK4 "
+                               "steps, checkpointed adjoint, FP64)",
                    "server": "4 streams, 32768-point chunks, <= 16 admitted requests, memory budget 50% free"},
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                        "max": float(lat.max())},
         "one_by_one_fp64": {"value": seq}, "speedup_vs_one_by_one_fp64": served / seq,
-        "server_stats": stats, "total_point_steps": point_steps,
+        "server_stats": stats, "total_point_steps": point_steps, "fit_requests": len(fit_idx),
+        "fit_gradient_check": fit_check,
     }
     print(json.dumps(line))
     return 0

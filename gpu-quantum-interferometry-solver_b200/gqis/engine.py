@@ -13,6 +13,7 @@ from __future__ import annotations
 import ctypes
 import hashlib
 import os
+import re
 import shutil
 import subprocess
 import tempfile
@@ -59,22 +60,42 @@ def nvcc_path() -> str:
                        "(set GQIS_NVCC or put CUDA's bin directory on PATH).")
 
 
-def _templates_digest() -> str:
-    h = hashlib.sha256()
-    for path in sorted(list(CSRC_DIR.glob("*.cuh")) + list(INCLUDE_DIR.glob("*.h"))):
-        h.update(path.name.encode())
-        h.update(path.read_bytes())
-    return h.hexdigest()
+_INCLUDE_RE = re.compile(r'^\s*#\s*include\s+"([^"]+)"', re.M)
+_DIGESTS: dict = {}
 
 
-_TEMPLATE_DIGEST = None
+def _header_path(name: str):
+    for base in (CSRC_DIR, INCLUDE_DIR):
+        if (base / name).exists():
+            return base / name
+    return None
 
 
-def templates_digest() -> str:
-    global _TEMPLATE_DIGEST
-    if _TEMPLATE_DIGEST is None:
-        _TEMPLATE_DIGEST = _templates_digest()
-    return _TEMPLATE_DIGEST
+def templates_digest(source: str) -> str:
+    """Hash of the headers ``source`` includes from csrc/ and include/, followed transitively.
+
+    A module's cache key depends only on the templates it is built from, so a change to one
+    integrator header leaves modules of the other integrators valid.
+    """
+    names, todo = set(), _INCLUDE_RE.findall(source)
+    while todo:
+        name = todo.pop()
+        if name in names:
+            continue
+        names.add(name)
+        path = _header_path(name)
+        if path is not None:
+            todo.extend(_INCLUDE_RE.findall(path.read_text()))
+    key = tuple(sorted(names))
+    digest = _DIGESTS.get(key)
+    if digest is None:
+        h = hashlib.sha256()
+        for name in key:
+            path = _header_path(name)
+            h.update(name.encode())
+            h.update(path.read_bytes() if path is not None else b"<system>")
+        digest = _DIGESTS[key] = h.hexdigest()
+    return digest
 
 
 def module_source(frag, spec, form, output_mode, trace_mode, unroll=False, extra_code="", defines=None):
@@ -132,7 +153,7 @@ class ModelModule:
 def build_module(source: str, *, extra_flags=(), quiet=True) -> Path:
     """Compile ``source`` into a cached shared library; returns its path."""
     flags = tuple(extra_flags)
-    key = hashlib.sha256((source + "\0" + templates_digest() + "\0" + " ".join(flags)).encode()).hexdigest()[:24]
+    key = hashlib.sha256((source + "\0" + templates_digest(source) + "\0" + " ".join(flags)).encode()).hexdigest()[:24]
     out_dir = cache_dir()
     so_path = out_dir / f"gqis_model_{key}.so"
     if so_path.exists():
