@@ -384,6 +384,69 @@ def run_duffing(args):
     return 0
 
 
+def run_hilbert(args):
+    """Config C4: Hilbert-space scaling of the density-matrix kernel, N in {8, 16, 32, 64}, 64 x 64
+    (eps, A) points, 2000 RK4 steps on [0, 100]; FP64 and FP32 forms, error vs the FP64 oracle."""
+    import numpy as np
+    import torch
+    torch.cuda.set_device(0)
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import lindblad_oracle
+    from gqis import native, solver, workloads
+    peaks = {"fp64": native.probe_fma_tflops(0), "fp32": native.probe_fma_tflops(1)}
+    dims = tuple(int(n) for n in args.dims.split(","))
+    flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    rows = {}
+    sampler = ClockSampler(0).start()
+    for N in dims:
+        w = workloads.n_level(N, side=64, steps=2000, duration=100.0)
+        model = (w["H"], w["Drive"], w["Col_Ops"], w["mean_operator"], w["tlist"])
+        points, steps = 64 * 64, 2000
+        forms = [("matrix", "fp64"), ("matrix", "fp32")] + ([("reduced", "fp64"), ("reduced", "fp32")] if N <= 8 else [])
+        maps, row = {}, {}
+        for rhs_form, prec in forms:
+            sweep = solver.prepare_sweep("mesolve_2D", *model, var_arrays=w["var_arrays"], precision=prec,
+                                         rhs_form=rhs_form)
+            reps = 1 if N >= 64 else max(1, args.steps // 2)
+            ms = float(np.mean(time_launches(torch, sweep, reps, 1, flush)))
+            flops = sweep.flops_per_point_step() * points * steps
+            rate = flops / (ms / 1e3) / 1e12
+            maps[(rhs_form, prec)] = sweep.results.double().cpu().numpy()
+            row[f"{rhs_form}_{prec}"] = {"ms": ms, "points_steps_per_s": points * steps / (ms / 1e3),
+                                         "flops_per_point_step": sweep.flops_per_point_step(),
+                                         "tflops": rate, "frac_of_measured_fma_peak": rate / peaks[prec]}
+            del sweep
+        # the FP64 oracle on 4 points of the grid (full 2000 steps)
+        eps, A = w["symbols"]
+        idx = np.array([0, 21, 42, 63])
+        sub = {eps: np.asarray(w["var_arrays"][eps])[idx[:2]], A: np.asarray(w["var_arrays"][A])[idx[2:]]}
+        ref = lindblad_oracle.rk4_sweep(lindblad_oracle.from_workload(w, sub), w["tlist"]).reshape(-1)
+        sel = (idx[:2][:, None] * 64 + idx[2:][None, :]).reshape(-1)
+        for key, m in maps.items():
+            got = m[sel, 0] + 1j * m[sel, 1]
+            row[f"{key[0]}_{key[1]}"]["max_abs_err_vs_fp64_oracle_4pts"] = float(np.max(np.abs(got - ref)))
+        full64 = maps[("matrix", "fp64")]
+        row["matrix_fp32"]["max_abs_vs_matrix_fp64_full_map"] = float(np.max(np.abs(maps[("matrix", "fp32")] - full64)))
+        row["fp32_speedup_vs_fp64"] = row["matrix_fp64"]["ms"] / row["matrix_fp32"]["ms"]
+        rows[N] = row
+    clocks = sampler.stop()
+    head = rows[16 if 16 in rows else dims[0]]
+    line = {
+        "metric": "points*steps/s (RK4 density-matrix kernel, N-level scaling model; FP32 form, N=16 headline)",
+        "value": head["matrix_fp32"]["points_steps_per_s"], "unit": "points*steps/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": 1, "ms_per_step": head["matrix_fp32"]["ms"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "N-level model: H0 seeded GUE-like + eps diag(0..N-1) + A cos(t) X; N-1 lowering "
+                               "ops at rate 0.01, N dephasing ops at rate 0.005; 64x64 (eps, A) grid, 2000 RK4 "
+                               "steps on [0, 100], mean <|N-1><N-1|>", "dims": list(dims),
+                   "l2": "flushed (256 MiB write) between timed launches"},
+        "per_dimension": {str(k): v for k, v in rows.items()},
+        "measured_fma_peaks_tflops": peaks, "clocks": clocks,
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def run_serving(args):
     """Config C5 (sweeps): Poisson stream of mixed-N, mixed-size sweep requests through the
     continuous-batching server (FP32 form), against the same requests one by one on plain FP64."""
@@ -500,7 +563,8 @@ def main():
     ap.add_argument("--requests", type=int, default=48, help="serving: number of requests")
     ap.add_argument("--rate", type=float, default=50.0, help="serving: Poisson arrival rate (1/s)")
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--workload", default="four_level", choices=("four_level", "duffing", "serving"),
+    ap.add_argument("--dims", default="8,16,32,64", help="hilbert: Hilbert-space dimensions")
+    ap.add_argument("--workload", default="four_level", choices=("four_level", "duffing", "serving", "hilbert"),
                     help="four_level: the headline RK4 interferogram; duffing: the adaptive ODE sweep")
     ap.add_argument("--solver", default="dop853a", help="adaptive solver of --workload duffing")
     args = ap.parse_args()
@@ -510,6 +574,8 @@ def main():
         return run_duffing(args)
     if args.workload == "serving":
         return run_serving(args)
+    if args.workload == "hilbert":
+        return run_hilbert(args)
     return run_ours(args)
 
 

@@ -14,7 +14,7 @@ OPTION_GROUPS = {
     "initial": ("rho0", "rho0_var_arrays", "rho0_values", "y0_values", "t_in"),
     "output": ("warmup_time", "return_time_trace", "time_trace_every", "time_trace_samples_per_period",
                "solver_samples_per_period", "return_device"),
-    "solver_options": ("solver", "fp64", "solver_frequency", "adaptive_options", "precision"),
+    "solver_options": ("solver", "fp64", "solver_frequency", "adaptive_options", "precision", "rhs_form"),
     "codegen": ("RHSreuse", "kernel_template_file", "unroll", "pre_expand", "collect_rho", "factor_terms",
                 "cse_batch_size", "cse_simplify", "hoist_rho_independent", "symbolic_workers",
                 "max_symbolic_workers", "nvrtc_options"),

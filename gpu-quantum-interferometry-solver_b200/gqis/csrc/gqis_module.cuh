@@ -19,8 +19,13 @@
 #include "gqis_adaptive.cuh"
 #include "gqis_adjoint.cuh"
 
+#include <type_traits>
+
 #ifndef GQ_WITH_ADJOINT
 #define GQ_WITH_ADJOINT 0
+#endif
+#ifndef GQ_MATRIX
+#define GQ_MATRIX 0
 #endif
 
 namespace {
@@ -42,10 +47,20 @@ int cuda_fail(cudaError_t e, const char* what) {
 using Model = GQ_MODEL;
 using Form = GQ_FORM;
 
-#if GQ_ADAPTIVE
+#if GQ_MATRIX
+// Density-matrix form (gqis_matrix.cuh, included by the generated source): one CTA per point.
+constexpr auto kKernel = gqmatrix::matrix_rk4_kernel<Model, Form, GQ_OUT>;
+constexpr int kBlock = Model::THREADS;
+constexpr size_t kSmem = gqmatrix::smem_bytes<Model, typename Form::real>();
+static_assert(std::is_same<typename Model::real, typename Form::real>::value, "model data type");
+#elif GQ_ADAPTIVE
 constexpr auto kKernel = gqadaptive::sweep_adaptive_kernel<GQ_SOLVER, Model, Form, GQ_OUT, GQ_TRACE>;
+constexpr int kBlock = GQ_BLOCK;
+constexpr size_t kSmem = 0;
 #else
 constexpr auto kKernel = gqfixed::sweep_fixed_kernel<GQ_SOLVER, Model, Form, GQ_OUT, GQ_TRACE>;
+constexpr int kBlock = GQ_BLOCK;
+constexpr size_t kSmem = 0;
 #endif
 
 int check_desc(const gqis_sweep_desc* d) {
@@ -97,7 +112,7 @@ __attribute__((visibility("default"))) int gqis_model_info_get(gqis_model_info* 
     out->output_mode = GQ_OUT;
     out->trace_mode = GQ_TRACE;
     out->init_from_array = Model::kInitFromArray ? 1 : 0;
-    out->block_threads = GQ_BLOCK;
+    out->block_threads = kBlock;
     out->model_hash = (uint64_t)GQ_MODEL_HASH;
     out->registers_per_thread = 0;
     out->sm_count = 0;
@@ -110,7 +125,7 @@ __attribute__((visibility("default"))) int gqis_model_info_get(gqis_model_info* 
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
         return cuda_fail(e, "cudaDeviceGetAttribute");
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas, kKernel, GQ_BLOCK, 0)) != cudaSuccess)
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas, kKernel, kBlock, kSmem)) != cudaSuccess)
         return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
     out->sm_count = sms;
     out->ctas_per_sm = ctas;
@@ -121,7 +136,14 @@ __attribute__((visibility("default"))) int gqis_sweep_launch(const gqis_sweep_de
     int rc = check_desc(d);
     if (rc != GQIS_OK || d->point_count == 0) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-#if GQ_ADAPTIVE
+#if GQ_MATRIX
+    cudaError_t e;
+    if (kSmem > 48 * 1024 &&
+        (e = cudaFuncSetAttribute(kKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem)) != cudaSuccess)
+        return cuda_fail(e, "cudaFuncSetAttribute(max dynamic shared memory)");
+    if (d->point_count > 0x7fffffffLL) return fail(GQIS_ERR_TOO_LARGE, "too many points for one launch");
+    kKernel<<<(unsigned)d->point_count, kBlock, kSmem, st>>>(*d);
+#elif GQ_ADAPTIVE
     // Persistent grid: every resident CTA slot of the device, lanes refill themselves.
     int dev = 0, sms = 0, ctas = 0;
     cudaError_t e;

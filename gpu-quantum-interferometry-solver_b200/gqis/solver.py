@@ -56,6 +56,7 @@ _CALIBRATION_MAX_HALVINGS = 6
 TIMESTEP_CALIBRATION_ODE_DEFAULTS = {"rms_atol": 1e-4, "max_atol": 1e-3}
 
 PRECISIONS = ("fp64", "fp32")
+MATRIX_FORM_FROM = 16  # rhs_form="auto" switches to the density-matrix kernel from this dimension
 
 
 def _compile_rhs(*args, **kwargs):
@@ -224,8 +225,9 @@ class PreparedSweep:
         self.steps = int(launch.num_steps)
         frag = launch.entry["frag"]
         self.state_size = frag["state_size"]
-        self.rhs_flops = emit.count_rhs_flops(frag)
-        self.drive_flops = emit.count_drive_flops(frag)
+        self.matrix = bool(frag.get("matrix"))
+        self.rhs_flops = None if self.matrix else emit.count_rhs_flops(frag)
+        self.drive_flops = None if self.matrix else emit.count_drive_flops(frag)
         self.solver = launch.entry["spec"].name
 
     @property
@@ -244,6 +246,8 @@ class PreparedSweep:
 
     def flops_per_point_step(self):
         """Algorithmic flops per point and RK4 step: 4 RHS + stage updates + 2 drive sets + <O>."""
+        if self.matrix:
+            return self.launch_spec.entry["frag"]["flops_per_point_step"]
         S = self.state_size
         return 4 * self.rhs_flops + 13 * S + 2 * self.drive_flops + 4
 
@@ -348,8 +352,8 @@ def mesolve_2D(H, Drive=None, Col_Ops=None, mean_operator=None, tlist=None,
                time_trace_samples_per_period=None, solver_samples_per_period=None,
                Actual_Kernel_Save=False, beep_on_error=False, ignore_non_finite_output=False,
                t_in=0.0, return_device=False, calibrate_timesteps=None, consts=None, initial=None,
-               output=None, solver_options=None, codegen=None, diagnostics=None, _prebuild_only=False,
-               _prepare_only=None):
+               output=None, solver_options=None, codegen=None, diagnostics=None, rhs_form="auto",
+               _prebuild_only=False, _prepare_only=None):
     args = dict(locals())
     groups = {name: args.pop(name) for name in OPTION_GROUPS}
     args, _ = apply_option_groups(mesolve_2D, args, groups)
@@ -387,7 +391,7 @@ def _solve_symbolic_system(H, Drive, Col_Ops, mean_operator, tlist,
                            Actual_Kernel_Save=False, beep_on_error=False, ignore_non_finite_output=False,
                            t_in=0.0, return_device=False, calibrate_timesteps=None, compiled_rhs=None,
                            _ode_size=None, _state_trace=False, _time_trace_offset=0, _prebuild_only=False,
-                           _prepare_only=None):
+                           _prepare_only=None, rhs_form="auto"):
     """Solve a Lindblad master equation (or, through ``odesolve_2D``, a real ODE) on a 1-D or 2-D
     parameter sweep, one independent time integration per point on the GPU.
 
@@ -401,8 +405,11 @@ def _solve_symbolic_system(H, Drive, Col_Ops, mean_operator, tlist,
     * ``return_device=True`` returns torch CUDA tensors instead of NumPy arrays.
 
     Additions of this engine: ``precision`` (``"fp64"`` or ``"fp32"``; default from ``fp64``),
-    the adaptive ``"dop853a"`` solver, and ``kernel_template_file``, which here names an extra
-    include directory (or a file in it) searched before the packaged CUDA templates.
+    the adaptive ``"dop853a"`` solver, ``kernel_template_file``, which here names an extra
+    include directory (or a file in it) searched before the packaged CUDA templates, and
+    ``rhs_form``: ``"reduced"`` (the reference's N*N-1 real equations), ``"matrix"`` (the
+    density-matrix kernel of ``matrix_form``; fixed-step RK4, outputs ``mean``/``final``/
+    ``final_rho``, no time trace) or ``"auto"`` (matrix from N = 16 on where it applies).
     """
     if (calibrate_timesteps is not None and calibrate_timesteps is not False and not _prebuild_only
             and _prepare_only is None):
@@ -511,8 +518,24 @@ def _solve_symbolic_system(H, Drive, Col_Ops, mean_operator, tlist,
     collect = bool(timings or return_timing_info)
     t_total = time.time()
 
+    if rhs_form not in ("auto", "reduced", "matrix"):
+        raise ValueError("rhs_form must be 'auto', 'reduced' or 'matrix'.")
+    matrix_ok = (compiled_rhs is None and _ode_size is None and spec.name == "rk4" and not return_time_trace
+                 and mode in ("mean", "final", "final_rho"))
+    if rhs_form == "matrix" and not matrix_ok:
+        raise ValueError("rhs_form='matrix' needs a Lindblad model given symbolically, solver='rk4', "
+                         "output_mode 'mean', 'final' or 'final_rho' and no time trace.")
+    use_matrix = rhs_form == "matrix" or (rhs_form == "auto" and matrix_ok and H is not None
+                                          and H.shape[0] >= MATRIX_FORM_FROM)
+
     # ---- 1) symbolic preparation
-    if compiled_rhs is None:
+    if use_matrix:
+        from . import matrix_form
+        compiled, rhs_status = matrix_form.compile_matrix_model(
+            H, Drive, Col_Ops, mean_operator, sweep_symbols=tuple(var_arrays), const_values=const_values,
+            runtime_consts=runtime_consts, keep_symbolic_consts=keep_symbolic_consts,
+            auto_runtime_consts=auto_runtime_consts, rho0=rho0, reuse=RHSreuse)
+    elif compiled_rhs is None:
         compiled, rhs_status = _compile_rhs(
             H, Drive, Col_Ops, mean_operator, sweep_symbols=tuple(var_arrays), const_values=const_values,
             runtime_consts=runtime_consts, keep_symbolic_consts=keep_symbolic_consts,
@@ -523,14 +546,22 @@ def _solve_symbolic_system(H, Drive, Col_Ops, mean_operator, tlist,
             symbolic_workers=symbolic_workers, max_symbolic_workers=max_symbolic_workers)
     else:
         compiled, rhs_status = compiled_rhs, "provided"
-    stages = (dict(compiled.timings) if rhs_status == "miss" else {"ode_prepare_s": 0.0, "ode_optimize_s": 0.0})
+    if use_matrix:
+        stages = {"ode_prepare_s": time.time() - t_total, "ode_optimize_s": 0.0}
+    else:
+        stages = (dict(compiled.timings) if rhs_status == "miss" else {"ode_prepare_s": 0.0, "ode_optimize_s": 0.0})
     const_vals = runtime_const_values(compiled, runtime_consts, const_values,
                                       use_defaults=compiled_rhs is not None)
 
     # ---- 2) model emission
     t0 = time.time()
     ekey = ("b200", bool(uses_rho0_values))
-    if RHSreuse and ekey in compiled.emitted:
+    if use_matrix:
+        frag = {"matrix": True, "state_size": compiled.state_size,
+                "used_const_indices": tuple(range(len(const_vals))),
+                "flops_per_point_step": matrix_form.flops_per_point_step(compiled), "dimension": compiled.Np}
+        stages["emit_s"] = 0.0
+    elif RHSreuse and ekey in compiled.emitted:
         frag, stages["emit_s"] = compiled.emitted[ekey], 0.0
     else:
         frag = emit.emit_model(compiled, uses_rho0_values)
@@ -547,13 +578,15 @@ def _solve_symbolic_system(H, Drive, Col_Ops, mean_operator, tlist,
         flags = (f"-I{template_dir}",) + flags
     tmtime = os.path.getmtime(kernel_template_file) if kernel_template_file else None
     kkey = ("b200_kernel_v1", compiled.cache_key, bool(uses_rho0_values), mode, spec.name, unroll,
-            form, trace_mode, flags, tmtime)
+            form, trace_mode, flags, tmtime, use_matrix)
     kernel_status = "miss"
     t_build = time.time()
     entry = _KERNEL_CACHE.get(kkey) if RHSreuse else None
     if entry is None:
         from . import engine
-        entry = {"source": engine.module_source(frag, spec, form, mode, trace_mode, unroll),
+        source = (matrix_form.module_source(compiled, form, mode, bool(uses_rho0_values)) if use_matrix
+                  else engine.module_source(frag, spec, form, mode, trace_mode, unroll))
+        entry = {"source": source,
                  "module": None, "flags": flags + (("-DGQ_FULL_UNROLL=1",) if unroll else ()),
                  "frag": frag, "spec": spec, "compiled": compiled}
         if RHSreuse:
@@ -665,7 +698,8 @@ def _solve_symbolic_system(H, Drive, Col_Ops, mean_operator, tlist,
                 "ode_optimize_s": stages["ode_optimize_s"], "code_emit_s": stages["emit_s"],
                 "kernel_build_s": stage_build, "cached_rhs": rhs_status, "cached_kernel": kernel_status,
                 "solver": spec.name, "solver_frequency": solver_frequency, "unroll": unroll,
-                "precision": form, "rhs_flops": emit.count_rhs_flops(frag)}
+                "precision": form, "rhs_form": "matrix" if use_matrix else "reduced",
+                "rhs_flops": None if use_matrix else emit.count_rhs_flops(frag)}
         module = entry.get("module")
         if hasattr(module, "info"):
             mi = module.info()

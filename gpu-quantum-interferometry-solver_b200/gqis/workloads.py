@@ -98,7 +98,12 @@ def duffing(side=None, full=1024, duration=500.0, intervals=512, seed=0):
 
 
 def n_level(N, side=64, steps=2000, duration=100.0, seed=0):
-    """N-level scaling model; matrices are numeric (seeded) and returned with the SymPy model."""
+    """N-level scaling model; matrices are numeric (seeded) and returned with the SymPy model.
+
+    eps spans [-0.5, 0.5]: the level spread eps (N-1) then stays below 32 at N = 64, so that
+    the largest transition frequency times dt = 0.05 (about 2) lies inside RK4's stability
+    interval on the imaginary axis (|omega dt| < 2.83); with eps in [-1, 1] RK4 diverges at N = 64.
+    """
     eps, A, Drive, t = sp.symbols("eps A Drive t", real=True)
     rng = np.random.default_rng(seed + N)
     G = (rng.normal(size=(N, N)) + 1j * rng.normal(size=(N, N))) / np.sqrt(2 * N)
@@ -120,6 +125,6 @@ def n_level(N, side=64, steps=2000, duration=100.0, seed=0):
     O[N - 1, N - 1] = 1
     return {"name": f"n_level_{N}", "H": H, "Drive": A * sp.cos(t), "Col_Ops": col, "mean_operator": O,
             "tlist": np.linspace(0.0, duration, steps + 1),
-            "var_arrays": {eps: np.linspace(-1.0, 1.0, side), A: np.linspace(0.0, 2.0, side)},
+            "var_arrays": {eps: np.linspace(-0.5, 0.5, side), A: np.linspace(0.0, 2.0, side)},
             "const_values": {}, "symbols": (eps, A), "N": N, "H0": H0, "X": X, "D": D,
             "lowering_rate": 0.01, "dephasing_rate": 0.005, "omega": 1.0}

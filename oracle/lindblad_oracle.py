@@ -70,6 +70,21 @@ class MatrixModel:
             Hs[p] = np.array(self.static_fn(*[a[p] for a in self.params]), dtype=complex)
         self.H_static = Hs
         self.LdL = sum((L.conj().T @ L for L in self.L), np.zeros((self.N, self.N), dtype=complex))
+        # L rho L^dag of sparse collapse operators as one sparse map on row-major vec(rho):
+        # (L rho L^dag)_ij = sum_ab L_ia rho_ab conj(L_jb); dense operators stay as products.
+        import scipy.sparse as sps
+        rows, cols, vals, self.L_dense = [], [], [], []
+        for L in self.L:
+            nz = list(zip(*np.nonzero(L)))
+            if len(nz) ** 2 > 4 * self.N * self.N:
+                self.L_dense.append(L)
+                continue
+            for (i, a) in nz:
+                for (j, b) in nz:
+                    rows.append(i * self.N + j)
+                    cols.append(a * self.N + b)
+                    vals.append(L[i, a] * np.conj(L[j, b]))
+        self.jump_T = sps.csr_matrix((np.array(vals, dtype=complex), (cols, rows)), shape=(self.N**2,) * 2)
         # Row-major vectorisation, vec(A rho B) = (A kron B^T) vec(rho): for small N the RHS is a
         # per-point superoperator applied to vec(rho) (same equation, far fewer NumPy calls).
         self.superop = self.N <= 8
@@ -100,10 +115,13 @@ class MatrixModel:
             for d, Md in zip(H, self.M_drive):
                 out += d[:, None] * (v @ Md.T)
             return out.reshape(rho.shape)
-        out = -1j * (H @ rho - rho @ H)
-        for L in self.L:
+        # -i[H, rho] - 1/2 {LdL, rho} = -i (Heff rho - rho Heff^dag), Heff = H - i/2 LdL
+        Heff = H - 0.5j * self.LdL
+        out = -1j * (Heff @ rho - rho @ np.conj(np.swapaxes(Heff, -1, -2)))
+        for L in self.L_dense:
             out += L @ rho @ L.conj().T
-        out -= 0.5 * (self.LdL @ rho + rho @ self.LdL)
+        P = rho.shape[0]
+        out += (rho.reshape(P, -1) @ self.jump_T).reshape(rho.shape)
         return out
 
     def observe(self, rho):

@@ -1,0 +1,81 @@
+"""GPU tests of the density-matrix (matrix-form) kernel, csrc/gqis_matrix.cuh.
+
+* FP64 against the reduced-form kernel on the same N = 8 model (two independent derivations of
+  one master equation): 1e-12 max-abs;
+* FP64 against the matrix-form CPU oracle (oracle/lindblad_oracle.py) at N = 16, 32, 64:
+  1e-11 max-abs on <O> maps whose entries are O(1e-5 .. 1);
+* the FP32 form against the same oracle: 2e-6 max-abs;
+* final_rho in the reduced layout, and rho0_values read back from it (a run split in two
+  equals the run in one piece);
+* rhs_form="auto" picks the matrix form from N = 16 on.
+"""
+
+import numpy as np
+import pytest
+
+import lindblad_oracle
+from test_support_calls import MATRIX_DIMS, hilbert_model, serving_model
+
+
+def _oracle(w, kwargs, output_mode="mean", rho0=None, t_in=0.0):
+    model = lindblad_oracle.from_workload(w, kwargs["var_arrays"])
+    return lindblad_oracle.rk4_sweep(model, w["tlist"], output_mode=output_mode, rho0=rho0, t_in=t_in)
+
+
+@pytest.mark.gpu
+def test_matrix_form_matches_reduced_form_n8():
+    import gqis
+    args, kwargs = serving_model(8, 6)
+    tl = np.linspace(0.0, 5.0, 101)
+    args = args[:4] + (tl,)
+    red = gqis.mesolve_2D(*args, **kwargs, fp64=True, rhs_form="reduced")
+    mat = gqis.mesolve_2D(*args, **kwargs, fp64=True, rhs_form="matrix")
+    assert np.max(np.abs(mat - red)) <= 1e-12
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("N", MATRIX_DIMS)
+def test_matrix_form_fp64_vs_oracle(N):
+    import gqis
+    w, args, kwargs = hilbert_model(N)
+    got, info = gqis.mesolve_2D(*args, **kwargs, fp64=True, rhs_form="matrix", return_timing_info=True)
+    assert info["rhs_form"] == "matrix"
+    ref = _oracle(w, kwargs)
+    assert np.max(np.abs(ref)) > 1e-5  # a non-trivial map (the top level fills slowly at N = 64)
+    err = float(np.max(np.abs(got - ref)))
+    assert err <= 1e-11, f"N={N}: FP64 matrix form max-abs error {err:.3e}"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("N", MATRIX_DIMS)
+def test_matrix_form_fp32_accuracy(N):
+    import gqis
+    w, args, kwargs = hilbert_model(N)
+    got = gqis.mesolve_2D(*args, **kwargs, precision="fp32", rhs_form="matrix")
+    err = float(np.max(np.abs(got - _oracle(w, kwargs))))
+    assert err <= 2e-6, f"N={N}: FP32 matrix form max-abs error {err:.3e}"
+
+
+@pytest.mark.gpu
+def test_matrix_form_final_rho_and_rho0_values_continuation():
+    import gqis
+    w, args, kwargs = hilbert_model(16)
+    full = gqis.mesolve_2D(*args, **kwargs, fp64=True, rhs_form="matrix", output_mode="final_rho")
+    ref = _oracle(w, kwargs, output_mode="final_rho")
+    assert full.shape == (4, 3, 255)
+    assert np.max(np.abs(full - ref)) <= 1e-11
+    tl = w["tlist"]
+    half = len(tl) // 2
+    first = gqis.mesolve_2D(*args[:4], tl[:half + 1], **kwargs, fp64=True, rhs_form="matrix",
+                            output_mode="final_rho")
+    second = gqis.mesolve_2D(*args[:4], tl[:len(tl) - half], **kwargs, fp64=True, rhs_form="matrix",
+                             output_mode="final_rho", rho0_values=first, t_in=float(tl[half]))
+    assert np.max(np.abs(second - full)) <= 1e-12
+
+
+@pytest.mark.gpu
+def test_auto_picks_matrix_form_from_n16():
+    import gqis
+    w, args, kwargs = hilbert_model(16)
+    _, info = gqis.mesolve_2D(*args, **kwargs, precision="fp32", return_timing_info=True)
+    assert info["rhs_form"] == "matrix"

@@ -38,6 +38,33 @@ def serving_model(N, side):
             {"var_arrays": var, "const_values": w["const_values"]})
 
 
+MATRIX_DIMS = (16, 32, 64)
+
+
+def hilbert_model(N, side=(4, 3), steps=100, duration=5.0):
+    """(workload, args, kwargs) of the N-level scaling model on a small grid (matrix-form tests)."""
+    W = ref_cases.workloads()
+    w = W.n_level(N, side=64, steps=steps, duration=duration)
+    eps, A = w["symbols"]
+    var = {eps: np.linspace(-0.5, 0.5, side[0]), A: np.linspace(0.0, 2.0, side[1])}
+    return w, (w["H"], w["Drive"], w["Col_Ops"], w["mean_operator"], w["tlist"]), {"var_arrays": var}
+
+
+def matrix_calls():
+    """Matrix-form module variants of the GPU tests and the Hilbert-space scaling benchmark."""
+    out = []
+    for N in (8,) + MATRIX_DIMS:
+        _, args, kwargs = hilbert_model(N)
+        for form in ("fp64", "fp32"):
+            out.append(("mesolve_2D", args, dict(kwargs, precision=form, rhs_form="matrix")))
+    _, args, kwargs = hilbert_model(16)
+    out.append(("mesolve_2D", args, dict(kwargs, fp64=True, rhs_form="matrix", output_mode="final_rho")))
+    rho0 = np.zeros((4, 3, 16 * 16 - 1))
+    out.append(("mesolve_2D", args, dict(kwargs, fp64=True, rhs_form="matrix", output_mode="final_rho",
+                                         rho0_values=rho0)))
+    return out
+
+
 def calls():
     out = []
     for N in (2, 4, 8):
