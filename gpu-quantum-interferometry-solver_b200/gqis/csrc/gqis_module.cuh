@@ -47,11 +47,19 @@ int cuda_fail(cudaError_t e, const char* what) {
 using Model = GQ_MODEL;
 using Form = GQ_FORM;
 
-#if GQ_MATRIX
+#if GQ_MATRIX == 2
+// Density-matrix form on the tensor cores (gqis_matrix_tc.cuh): one CTA per tile of 128 / N points.
+constexpr auto kKernel = gqmatrix_tc::matrix_tc_kernel<Model, GQ_OUT>;
+constexpr int kBlock = gqmatrix_tc::TcShape<Model>::THREADS;
+constexpr size_t kSmem = gqmatrix_tc::TcShape<Model>::SMEM;
+constexpr int kPointsPerCta = gqmatrix_tc::TcShape<Model>::P;
+static_assert(Form::id == GQIS_FORM_FP32, "the tensor-core form is an FP32 form");
+#elif GQ_MATRIX
 // Density-matrix form (gqis_matrix.cuh, included by the generated source): one CTA per point.
 constexpr auto kKernel = gqmatrix::matrix_rk4_kernel<Model, Form, GQ_OUT>;
 constexpr int kBlock = Model::THREADS;
 constexpr size_t kSmem = gqmatrix::smem_bytes<Model, typename Form::real>();
+constexpr int kPointsPerCta = 1;
 static_assert(std::is_same<typename Model::real, typename Form::real>::value, "model data type");
 #elif GQ_ADAPTIVE
 constexpr auto kKernel = gqadaptive::sweep_adaptive_kernel<GQ_SOLVER, Model, Form, GQ_OUT, GQ_TRACE>;
@@ -141,8 +149,9 @@ __attribute__((visibility("default"))) int gqis_sweep_launch(const gqis_sweep_de
     if (kSmem > 48 * 1024 &&
         (e = cudaFuncSetAttribute(kKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem)) != cudaSuccess)
         return cuda_fail(e, "cudaFuncSetAttribute(max dynamic shared memory)");
-    if (d->point_count > 0x7fffffffLL) return fail(GQIS_ERR_TOO_LARGE, "too many points for one launch");
-    kKernel<<<(unsigned)d->point_count, kBlock, kSmem, st>>>(*d);
+    const int64_t grid = (d->point_count + kPointsPerCta - 1) / kPointsPerCta;
+    if (grid > 0x7fffffffLL) return fail(GQIS_ERR_TOO_LARGE, "too many points for one launch");
+    kKernel<<<(unsigned)grid, kBlock, kSmem, st>>>(*d);
 #elif GQ_ADAPTIVE
     // Persistent grid: every resident CTA slot of the device, lanes refill themselves.
     int dev = 0, sms = 0, ctas = 0;

@@ -22,9 +22,10 @@ Floats in H are rounded to ten significant digits before the split, the conventi
 reference's code printer (``gqis/solver.py:166-170``); coefficient functions are printed by
 the same printer as the reduced form's model code.
 
-The CUDA kernel is ``csrc/gqis_matrix.cuh`` (one CTA per parameter point). The dimension is
-padded with inert levels to the kernel's tile (8, 16, 32, 48 or 64); padded levels have zero
-operators and zero population and stay exactly zero.
+The CUDA kernels are ``csrc/gqis_matrix.cuh`` (CUDA cores, one CTA per parameter point) and
+``csrc/gqis_matrix_tc.cuh`` (tensor cores, one CTA per 128 / N points). The dimension is padded
+with inert levels to the kernel's tile (8, 16, 32, 48 or 64); padded levels have zero operators
+and zero population and stay exactly zero.
 """
 
 from __future__ import annotations
@@ -373,23 +374,43 @@ def emit_matrix_model(mm: MatrixModel, form: str, uses_rho0_values: bool):
 
 
 OUTPUT_IDS = {"mean": 0, "final": 1, "final_rho": 2}
+TENSOR_DIMS = (8, 16, 32)
 
 
-def module_source(mm: MatrixModel, form: str, output_mode: str, uses_rho0_values: bool):
-    """Complete translation unit of one matrix-form module (C ABI of include/gqis_b200.h)."""
+def tensor_core_blockers(mm: MatrixModel, form: str):
+    """Reasons the tensor-core kernel (csrc/gqis_matrix_tc.cuh) cannot run this model; [] if it can."""
+    out = []
+    if form != "fp32":
+        out.append("the tensor-core form is an FP32 form (precision='fp32')")
+    if mm.Np not in TENSOR_DIMS:
+        out.append(f"padded dimension {mm.Np} is not one of {TENSOR_DIMS}")
+    elif 2 * mm.Np * (1 + mm.num_dense) > 256:
+        out.append(f"{mm.num_dense} time-dependent operator terms exceed one MMA (2 N (1 + terms) <= 256)")
+    if any(src // mm.Np != src % mm.Np for _, src, _, _ in mm.jumps):
+        out.append("a jump term reads an off-diagonal element (only populations may feed other elements)")
+    return out
+
+
+def module_source(mm: MatrixModel, form: str, output_mode: str, uses_rho0_values: bool, tensor_cores=False):
+    """Complete translation unit of one matrix-form module (C ABI of include/gqis_b200.h);
+    ``tensor_cores`` selects the tcgen05 kernel of csrc/gqis_matrix_tc.cuh."""
     if output_mode not in OUTPUT_IDS:
         raise ValueError(f"the matrix form supports the outputs {sorted(OUTPUT_IDS)}, not '{output_mode}'")
+    if tensor_cores:
+        blockers = tensor_core_blockers(mm, form)
+        if blockers:
+            raise ValueError("the tensor-core matrix form cannot run this model: " + "; ".join(blockers))
     model = emit_matrix_model(mm, form, uses_rho0_values)
     model_hash = int(hashlib.sha256(model.encode()).hexdigest()[:16], 16)
     form_type = {"fp64": "FormFP64", "fp32": "FormFP32"}[form]
     return "\n".join([
         "// Matrix-form model module generated by gqis (B200 sweep engine). Do not edit.",
         '#include "gqis_common.cuh"',
-        '#include "gqis_matrix.cuh"',
+        '#include "gqis_matrix_tc.cuh"' if tensor_cores else '#include "gqis_matrix.cuh"',
         "namespace gqmodel {",
         model,
         "}  // namespace gqmodel",
-        "#define GQ_MATRIX 1",
+        f"#define GQ_MATRIX {2 if tensor_cores else 1}",
         "#define GQ_MODEL gqmodel::MM",
         f"#define GQ_FORM {form_type}",
         "#define GQ_SOLVER_ID 0",
@@ -415,6 +436,13 @@ def flops_per_point_step(mm: MatrixModel):
     per_rhs = 8 * Np ** 3 + 4 * mm.num_dense * nn + (8 * nn + 4 * mm.num_diag * Np if mm.num_diag else 0)
     per_rhs += 2 * nn + 8 * nn + 8 * len(mm.jumps)
     return 4 * per_rhs + 26 * nn + 8 * nn
+
+
+def tensor_flops_per_point_step(mm: MatrixModel):
+    """Tensor-pipe arithmetic of one RK4 step of one point in the tcgen05 kernel: per RHS the
+    point's N rows of D (2 N (1 + ND) columns) over K = 2 N, three split-TF32 passes."""
+    Np = mm.Np
+    return 4 * 3 * 2 * Np * (2 * Np * (1 + mm.num_dense)) * (2 * Np)
 
 
 def dense_operators(mm: MatrixModel, X, Y, t, consts=()):

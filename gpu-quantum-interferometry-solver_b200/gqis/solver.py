@@ -408,8 +408,10 @@ def _solve_symbolic_system(H, Drive, Col_Ops, mean_operator, tlist,
     the adaptive ``"dop853a"`` solver, ``kernel_template_file``, which here names an extra
     include directory (or a file in it) searched before the packaged CUDA templates, and
     ``rhs_form``: ``"reduced"`` (the reference's N*N-1 real equations), ``"matrix"`` (the
-    density-matrix kernel of ``matrix_form``; fixed-step RK4, outputs ``mean``/``final``/
-    ``final_rho``, no time trace) or ``"auto"`` (matrix from N = 16 on where it applies).
+    density-matrix kernel of ``matrix_form`` on the CUDA cores; fixed-step RK4, outputs
+    ``mean``/``final``/``final_rho``, no time trace), ``"matrix_tc"`` (the same on the tensor
+    cores, split-TF32 operands with FP32 accumulation; FP32 form, padded N of 8, 16 or 32) or
+    ``"auto"`` (matrix from N = 16 on where it applies).
     """
     if (calibrate_timesteps is not None and calibrate_timesteps is not False and not _prebuild_only
             and _prepare_only is None):
@@ -518,15 +520,16 @@ def _solve_symbolic_system(H, Drive, Col_Ops, mean_operator, tlist,
     collect = bool(timings or return_timing_info)
     t_total = time.time()
 
-    if rhs_form not in ("auto", "reduced", "matrix"):
-        raise ValueError("rhs_form must be 'auto', 'reduced' or 'matrix'.")
+    if rhs_form not in ("auto", "reduced", "matrix", "matrix_tc"):
+        raise ValueError("rhs_form must be 'auto', 'reduced', 'matrix' or 'matrix_tc'.")
     matrix_ok = (compiled_rhs is None and _ode_size is None and spec.name == "rk4" and not return_time_trace
                  and mode in ("mean", "final", "final_rho"))
-    if rhs_form == "matrix" and not matrix_ok:
-        raise ValueError("rhs_form='matrix' needs a Lindblad model given symbolically, solver='rk4', "
+    if rhs_form in ("matrix", "matrix_tc") and not matrix_ok:
+        raise ValueError(f"rhs_form='{rhs_form}' needs a Lindblad model given symbolically, solver='rk4', "
                          "output_mode 'mean', 'final' or 'final_rho' and no time trace.")
-    use_matrix = rhs_form == "matrix" or (rhs_form == "auto" and matrix_ok and H is not None
-                                          and H.shape[0] >= MATRIX_FORM_FROM)
+    use_matrix = rhs_form in ("matrix", "matrix_tc") or (rhs_form == "auto" and matrix_ok and H is not None
+                                                         and H.shape[0] >= MATRIX_FORM_FROM)
+    tensor_cores = rhs_form == "matrix_tc"
 
     # ---- 1) symbolic preparation
     if use_matrix:
@@ -559,7 +562,9 @@ def _solve_symbolic_system(H, Drive, Col_Ops, mean_operator, tlist,
     if use_matrix:
         frag = {"matrix": True, "state_size": compiled.state_size,
                 "used_const_indices": tuple(range(len(const_vals))),
-                "flops_per_point_step": matrix_form.flops_per_point_step(compiled), "dimension": compiled.Np}
+                "flops_per_point_step": matrix_form.flops_per_point_step(compiled), "dimension": compiled.Np,
+                "tensor_cores": tensor_cores,
+                "tensor_flops_per_point_step": matrix_form.tensor_flops_per_point_step(compiled)}
         stages["emit_s"] = 0.0
     elif RHSreuse and ekey in compiled.emitted:
         frag, stages["emit_s"] = compiled.emitted[ekey], 0.0
@@ -578,13 +583,14 @@ def _solve_symbolic_system(H, Drive, Col_Ops, mean_operator, tlist,
         flags = (f"-I{template_dir}",) + flags
     tmtime = os.path.getmtime(kernel_template_file) if kernel_template_file else None
     kkey = ("b200_kernel_v1", compiled.cache_key, bool(uses_rho0_values), mode, spec.name, unroll,
-            form, trace_mode, flags, tmtime, use_matrix)
+            form, trace_mode, flags, tmtime, use_matrix, tensor_cores)
     kernel_status = "miss"
     t_build = time.time()
     entry = _KERNEL_CACHE.get(kkey) if RHSreuse else None
     if entry is None:
         from . import engine
-        source = (matrix_form.module_source(compiled, form, mode, bool(uses_rho0_values)) if use_matrix
+        source = (matrix_form.module_source(compiled, form, mode, bool(uses_rho0_values), tensor_cores)
+                  if use_matrix
                   else engine.module_source(frag, spec, form, mode, trace_mode, unroll))
         entry = {"source": source,
                  "module": None, "flags": flags + (("-DGQ_FULL_UNROLL=1",) if unroll else ()),
@@ -698,7 +704,8 @@ def _solve_symbolic_system(H, Drive, Col_Ops, mean_operator, tlist,
                 "ode_optimize_s": stages["ode_optimize_s"], "code_emit_s": stages["emit_s"],
                 "kernel_build_s": stage_build, "cached_rhs": rhs_status, "cached_kernel": kernel_status,
                 "solver": spec.name, "solver_frequency": solver_frequency, "unroll": unroll,
-                "precision": form, "rhs_form": "matrix" if use_matrix else "reduced",
+                "precision": form,
+                "rhs_form": ("matrix_tc" if tensor_cores else "matrix") if use_matrix else "reduced",
                 "rhs_flops": None if use_matrix else emit.count_rhs_flops(frag)}
         module = entry.get("module")
         if hasattr(module, "info"):

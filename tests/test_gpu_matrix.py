@@ -7,14 +7,17 @@
 * the FP32 form against the same oracle: 2e-6 max-abs;
 * final_rho in the reduced layout, and rho0_values read back from it (a run split in two
   equals the run in one piece);
-* rhs_form="auto" picks the matrix form from N = 16 on.
+* rhs_form="auto" picks the matrix form from N = 16 on;
+* the tensor-core kernel (split-TF32 tcgen05 MMAs, FP32 accumulation and state) against the same
+  oracle at N = 8, 16, 32: 5e-6 max-abs, and within 5e-6 of the CUDA-core FP32 form; final_rho
+  through it as well. The grids leave the last tile of points partly empty.
 """
 
 import numpy as np
 import pytest
 
 import lindblad_oracle
-from test_support_calls import MATRIX_DIMS, hilbert_model, serving_model
+from test_support_calls import MATRIX_DIMS, TENSOR_DIMS, hilbert_model, serving_model
 
 
 def _oracle(w, kwargs, output_mode="mean", rho0=None, t_in=0.0):
@@ -79,3 +82,27 @@ def test_auto_picks_matrix_form_from_n16():
     w, args, kwargs = hilbert_model(16)
     _, info = gqis.mesolve_2D(*args, **kwargs, precision="fp32", return_timing_info=True)
     assert info["rhs_form"] == "matrix"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("N", TENSOR_DIMS)
+def test_tensor_core_form_vs_oracle(N):
+    import gqis
+    w, args, kwargs = hilbert_model(N)
+    got, info = gqis.mesolve_2D(*args, **kwargs, precision="fp32", rhs_form="matrix_tc", return_timing_info=True)
+    assert info["rhs_form"] == "matrix_tc"
+    ref = _oracle(w, kwargs)
+    err = float(np.max(np.abs(got - ref)))
+    cuda = gqis.mesolve_2D(*args, **kwargs, precision="fp32", rhs_form="matrix")
+    assert err <= 5e-6, f"N={N}: tensor-core form max-abs error {err:.3e}"
+    assert float(np.max(np.abs(got - cuda))) <= 5e-6
+
+
+@pytest.mark.gpu
+def test_tensor_core_form_final_rho():
+    import gqis
+    w, args, kwargs = hilbert_model(16)
+    got = gqis.mesolve_2D(*args, **kwargs, precision="fp32", rhs_form="matrix_tc", output_mode="final_rho")
+    ref = _oracle(w, kwargs, output_mode="final_rho")
+    assert got.shape == ref.shape
+    assert float(np.max(np.abs(got - ref))) <= 5e-6

@@ -39,6 +39,7 @@ def serving_model(N, side):
 
 
 MATRIX_DIMS = (16, 32, 64)
+TENSOR_DIMS = (8, 16, 32)
 
 
 def hilbert_model(N, side=(4, 3), steps=100, duration=5.0):
@@ -57,7 +58,11 @@ def matrix_calls():
         _, args, kwargs = hilbert_model(N)
         for form in ("fp64", "fp32"):
             out.append(("mesolve_2D", args, dict(kwargs, precision=form, rhs_form="matrix")))
+    for N in TENSOR_DIMS:
+        _, args, kwargs = hilbert_model(N)
+        out.append(("mesolve_2D", args, dict(kwargs, precision="fp32", rhs_form="matrix_tc")))
     _, args, kwargs = hilbert_model(16)
+    out.append(("mesolve_2D", args, dict(kwargs, precision="fp32", rhs_form="matrix_tc", output_mode="final_rho")))
     out.append(("mesolve_2D", args, dict(kwargs, fp64=True, rhs_form="matrix", output_mode="final_rho")))
     rho0 = np.zeros((4, 3, 16 * 16 - 1))
     out.append(("mesolve_2D", args, dict(kwargs, fp64=True, rhs_form="matrix", output_mode="final_rho",
