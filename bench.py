@@ -399,11 +399,14 @@ def run_hilbert(args):
     rows = {}
     sampler = ClockSampler(0).start()
     for N in dims:
-        w = workloads.n_level(N, side=64, steps=2000, duration=100.0)
+        steps = args.hsteps
+        w = workloads.n_level(N, side=64, steps=steps, duration=100.0 * steps / 2000)
         model = (w["H"], w["Drive"], w["Col_Ops"], w["mean_operator"], w["tlist"])
-        points, steps = 64 * 64, 2000
+        points = 64 * 64
         forms = [("matrix", "fp64"), ("matrix", "fp32")] + ([("matrix_tc", "fp32")] if N <= 32 else []) + \
                 ([("reduced", "fp64"), ("reduced", "fp32")] if N <= 8 else [])
+        if args.forms:
+            forms = [f for f in forms if f"{f[0]}_{f[1]}" in args.forms.split(",")]
         maps, row = {}, {}
         for rhs_form, prec in forms:
             sweep = solver.prepare_sweep("mesolve_2D", *model, var_arrays=w["var_arrays"], precision=prec,
@@ -429,10 +432,11 @@ def run_hilbert(args):
         for key, m in maps.items():
             got = m[sel, 0] + 1j * m[sel, 1]
             row[f"{key[0]}_{key[1]}"]["max_abs_err_vs_fp64_oracle_4pts"] = float(np.max(np.abs(got - ref)))
-        full64 = maps[("matrix", "fp64")]
-        row["matrix_fp32"]["max_abs_vs_matrix_fp64_full_map"] = float(np.max(np.abs(maps[("matrix", "fp32")] - full64)))
-        row["fp32_speedup_vs_fp64"] = row["matrix_fp64"]["ms"] / row["matrix_fp32"]["ms"]
-        if ("matrix_tc", "fp32") in maps:
+        full64 = maps.get(("matrix", "fp64"))
+        if full64 is not None and ("matrix", "fp32") in maps:
+            row["matrix_fp32"]["max_abs_vs_matrix_fp64_full_map"] = float(np.max(np.abs(maps[("matrix", "fp32")] - full64)))
+            row["fp32_speedup_vs_fp64"] = row["matrix_fp64"]["ms"] / row["matrix_fp32"]["ms"]
+        if full64 is not None and ("matrix", "fp32") in maps and ("matrix_tc", "fp32") in maps:
             row["matrix_tc_fp32"]["max_abs_vs_matrix_fp64_full_map"] = float(
                 np.max(np.abs(maps[("matrix_tc", "fp32")] - full64)))
             row["tensor_core_speedup_vs_fp64"] = row["matrix_fp64"]["ms"] / row["matrix_tc_fp32"]["ms"]
@@ -440,7 +444,7 @@ def run_hilbert(args):
         rows[N] = row
     clocks = sampler.stop()
     head = rows[16 if 16 in rows else dims[0]]
-    hk = "matrix_tc_fp32" if "matrix_tc_fp32" in head else "matrix_fp32"
+    hk = "matrix_tc_fp32" if "matrix_tc_fp32" in head else sorted(k for k in head if isinstance(head[k], dict))[0]
     line = {
         "metric": "points*steps/s (RK4 density-matrix sweep, N-level scaling model; tensor-core split-TF32 "
                   "form, N=16 headline)",
@@ -448,8 +452,8 @@ def run_hilbert(args):
         "steps": args.steps, "warmup": 1, "ms_per_step": head[hk]["ms"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "N-level model: H0 seeded GUE-like + eps diag(0..N-1) + A cos(t) X; N-1 lowering "
-                               "ops at rate 0.01, N dephasing ops at rate 0.005; 64x64 (eps, A) grid, 2000 RK4 "
-                               "steps on [0, 100], mean <|N-1><N-1|>", "dims": list(dims),
+                               "ops at rate 0.01, N dephasing ops at rate 0.005; 64x64 (eps, A) grid, "
+                               f"{args.hsteps} RK4 steps of dt 0.05, mean <|N-1><N-1|>", "dims": list(dims),
                    "l2": "flushed (256 MiB write) between timed launches"},
         "per_dimension": {str(k): v for k, v in rows.items()},
         "measured_fma_peaks_tflops": peaks, "clocks": clocks,
@@ -575,6 +579,8 @@ def main():
     ap.add_argument("--rate", type=float, default=50.0, help="serving: Poisson arrival rate (1/s)")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--dims", default="8,16,32,64", help="hilbert: Hilbert-space dimensions")
+    ap.add_argument("--forms", default="", help="hilbert: comma list of forms to run (e.g. matrix_tc_fp32); all if empty")
+    ap.add_argument("--hsteps", type=int, default=2000, help="hilbert: RK4 steps (t spans 100 * hsteps / 2000)")
     ap.add_argument("--workload", default="four_level", choices=("four_level", "duffing", "serving", "hilbert"),
                     help="four_level: the headline RK4 interferogram; duffing: the adaptive ODE sweep")
     ap.add_argument("--solver", default="dop853a", help="adaptive solver of --workload duffing")

@@ -6,22 +6,25 @@
 //
 //   row r = p*N + j  (point p of the tile, column j of its rho)  = tensor-memory lane r
 //   A[r][k]   = Re rho_p[k][j] (k < N),  Im rho_p[k-N][j] (k >= N)        (tensor memory)
-//   B[k][col] = real embedding of T_q^T for the operator terms T_0 = Heff0, T_q = M_q
-//               col = (2q + c) N + n, c = 0 (Re) / 1 (Im)                  (shared memory)
+//   B[k][col] = real embedding of T_q^T for the operator terms           (shared memory)
+//               T_0 = Heff0, T_q = M_q (dense, q = 1..ND), T_{ND+g} = diag(v_g) (g = 1..NG)
+//               col = (2q + c) N + n, c = 0 (Re) / 1 (Im)
 //   D[r][col] = Re/Im (T_q rho_p)[n][j]                                    (tensor memory)
 //
-// so one MMA chain gives every point's Heff0 rho and M_q rho at once; the epilogue forms
-// K = H_eff(t) rho with the point's FP64-evaluated coefficients, then -i (K - K^dag) through a
-// transposed read of K in shared memory, the jump terms, and the RK4 combination, and writes the
-// next stage input back into A. Operands are split TF32 (x = hi + lo, both TF32), three MMAs per
-// K step (hi*hi + hi*lo + lo*hi) with FP32 accumulation; the state is FP32 with the FP32 form's
+// One MMA chain gives every point's T_q rho at once; the epilogue forms K = sum_q c_q(t) T_q rho
+// with the point's FP64-evaluated coefficients (c_0 = 1), -i (K - K^dag) through a transposed
+// read of K in shared memory, the jump terms, and the RK4 combination, and writes the next stage
+// input back into A. Operands are split TF32 (x = hi + lo, both TF32), three MMAs per K step
+// (hi*hi + hi*lo + lo*hi) with FP32 accumulation; the state is FP32 with the FP32 form's
 // compensated update, time and coefficients FP64, the mean of <O> FP64.
 //
-// Thread t: lane r = t % 128 of warp quadrant r / 32, rows n0 = 8 (t / 128) .. n0 + 7 of column j.
-// Jump sources must be diagonal elements (rho_aa, shared through `rdiag`); element-wise jump
-// terms and the diagonal H terms read the stage input back from A (hi + lo).
-// Every mbarrier wait is bounded: on give-up the CTA writes NaN outputs, waits (bounded) for
-// the MMA in flight, frees its tensor memory and returns.
+// Thread t: lane r = t % 128 (warp quadrant r / 32), rows n0 = 8 (t / 128) .. n0 + 7 of column j.
+// Coefficients are evaluated once per point and stage time by one thread and shared through
+// shared memory. Jump terms come from per-thread lists (the module's tcj_* tables) whose sources
+// are populations rho_aa, shared through shared memory when the stage input is written; element-
+// wise terms off the diagonal (kWOffDiag) read the stage input back from A (hi + lo).
+// Every mbarrier wait is bounded: on give-up the CTA writes NaN outputs, waits (bounded) for the
+// MMA in flight, frees its tensor memory and returns.
 #pragma once
 
 #include <type_traits>
@@ -44,10 +47,11 @@ struct TcShape {
     static constexpr int H = N / E;           // threads per column
     static constexpr int THREADS = 128 * H;
     static constexpr int MIN_CTAS = 65536 / (THREADS * 128);  // keeps <= 128 registers per thread
-    static constexpr int NT = 1 + MM::ND;     // operator terms in B
+    static constexpr int NT = 1 + MM::ND + MM::NG;  // operator terms in B
     static constexpr int NMMA = 2 * N * NT;   // B / D columns
     static constexpr int KDIM = 2 * N;        // real-embedded inner dimension
     static constexpr int KCH = KDIM / 8;      // MMA K steps of 8 TF32
+    static constexpr int NC = MM::NCOEF > 0 ? MM::NCOEF : 1;
     static constexpr int COL_D = 0, COL_AHI = NMMA, COL_ALO = NMMA + KDIM;
     static constexpr int COLS_USED = NMMA + 2 * KDIM;
     static constexpr int TMEM_COLS = COLS_USED <= 32 ? 32 : COLS_USED <= 64 ? 64 : COLS_USED <= 128 ? 128
@@ -58,9 +62,11 @@ struct TcShape {
     static constexpr size_t OFF_BHI = 0, OFF_BLO = B_BYTES;
     static constexpr size_t OFF_K = 2 * B_BYTES;
     static constexpr size_t K_BYTES = (size_t)P * N * LDK * 8;
-    static constexpr size_t OFF_RD = OFF_K + K_BYTES;
-    static constexpr size_t RD_BYTES = (size_t)P * N * 8;
-    static constexpr size_t OFF_RED = OFF_RD + RD_BYTES;
+    static constexpr size_t OFF_RD = OFF_K + K_BYTES;           // [2][P*N] populations of the stage input
+    static constexpr size_t RD_BYTES = 2 * (size_t)P * N * 4;
+    static constexpr size_t OFF_CS = OFF_RD + RD_BYTES;         // [2][P][NC] coefficients
+    static constexpr size_t CS_BYTES = 2 * (size_t)P * NC * 4;
+    static constexpr size_t OFF_RED = (OFF_CS + CS_BYTES + 7) / 8 * 8;
     static constexpr size_t RED_BYTES = 2 * (size_t)H * P * 8;
     static constexpr size_t OFF_MISC = OFF_RED + RED_BYTES;
     static constexpr size_t NEEDED = OFF_MISC + 64;
@@ -83,17 +89,24 @@ __device__ __forceinline__ uint32_t b_offset(int col, int k) {
     return (uint32_t)((k >> 3) * (T::NMMA * 32) + (col >> 3) * 256 + ((k & 7) >> 2) * 128 + (col & 7) * 16 + (k & 3) * 4);
 }
 
+// TF32 rounding (nearest, ties away from zero) of a finite FP32 number with integer operations:
+// add half a unit of the 10-bit mantissa's last place to the magnitude, clear the 13 dropped bits.
+__device__ __forceinline__ float tf32_round(float x) {
+    return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
+}
+
 template <class MM, int OUT>
 __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) matrix_tc_kernel(const gqis_sweep_desc d) {
     using T = TcShape<MM>;
     using F = FormFP32;
-    constexpr int N = T::N, P = T::P, E = T::E, LDK = T::LDK, NO = MM::NO;
+    constexpr int N = T::N, P = T::P, E = T::E, LDK = T::LDK, NO = MM::NO, NC = T::NC;
     static_assert(std::is_same<typename MM::real, float>::value, "tensor-core form uses FP32 model data");
     extern __shared__ __align__(1024) unsigned char gq_smem[];
     float* const bhi = reinterpret_cast<float*>(gq_smem + T::OFF_BHI);
     float* const blo = reinterpret_cast<float*>(gq_smem + T::OFF_BLO);
     Cx<float>* const kbuf = reinterpret_cast<Cx<float>*>(gq_smem + T::OFF_K);
-    Cx<float>* const rdiag = reinterpret_cast<Cx<float>*>(gq_smem + T::OFF_RD);
+    float* const rdiag = reinterpret_cast<float*>(gq_smem + T::OFF_RD);
+    float* const cs = reinterpret_cast<float*>(gq_smem + T::OFF_CS);
     double* const red = reinterpret_cast<double*>(gq_smem + T::OFF_RED);
     uint64_t* const bar = reinterpret_cast<uint64_t*>(gq_smem + T::OFF_MISC);
     uint32_t* const tslot = reinterpret_cast<uint32_t*>(gq_smem + T::OFF_MISC + 8);
@@ -105,6 +118,7 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
     const int n0 = hh * E;
     const int warp = tid >> 5;
     const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
+    const bool lead = (j == 0) && (hh == 0);  // evaluates the point's coefficients
 
     const int64_t local = (int64_t)blockIdx.x * P + p;
     const bool active = local < d.point_count;
@@ -113,9 +127,6 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
     const int ix = (int)(gp / d.num_y);
     const int iy = (int)(gp - (int64_t)ix * d.num_y);
     const double Xd = d.par_x[ix], Yd = d.par_y[iy];
-    double Cd[MM::NCONST];
-#pragma unroll
-    for (int i = 0; i < MM::NCONST; ++i) Cd[i] = d.consts ? __ldg(d.consts + i) : 0.0;
 
     // ---- B = split-TF32 real embedding of the operator terms; mbarrier; tensor memory
     for (int e = tid; e < T::NMMA * T::KDIM; e += T::THREADS) {
@@ -123,11 +134,19 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
         const int q = col / (2 * N), c = (col / N) & 1, n = col % N;
         const int m = k % N;
         const bool imag_in = k >= N;
-        const float* op = (q == 0) ? MM::heff() : MM::dense(q - 1);
-        const float tr = __ldg(op + 2 * (n * N + m)), ti = __ldg(op + 2 * (n * N + m) + 1);
-        const float v = (c == 0) ? (imag_in ? -ti : tr) : (imag_in ? tr : ti);
-        const float hi = gqtc::to_tf32(v);
-        const float lo = gqtc::to_tf32(v - hi);
+        float tr, ti;
+        if (q <= MM::ND) {
+            const float* op = (q == 0) ? MM::heff() : MM::dense(q - 1);
+            tr = __ldg(op + 2 * (n * N + m));
+            ti = __ldg(op + 2 * (n * N + m) + 1);
+        } else {
+            const float* v = MM::diag(q - 1 - MM::ND);
+            tr = (n == m) ? __ldg(v + 2 * n) : 0.f;
+            ti = (n == m) ? __ldg(v + 2 * n + 1) : 0.f;
+        }
+        const float val = (c == 0) ? (imag_in ? -ti : tr) : (imag_in ? tr : ti);
+        const float hi = tf32_round(val);
+        const float lo = tf32_round(val - hi);
         const uint32_t off = b_offset<T>(col, k) >> 2;
         bhi[off] = hi;
         blo[off] = lo;
@@ -183,25 +202,32 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
             are[e] = aim[e] = 0.f;
         }
     }
+    const int jl = j * T::H + hh;  // this thread's jump list
+    const int jcount = __ldg(MM::tcj_count() + jl);
 
-    double c[MM::NCOEF > 0 ? MM::NCOEF : 1];
-    float cr[MM::NCOEF > 0 ? MM::NCOEF : 1];
-    auto coef = [&](double t) {
-        MM::coef(t, Xd, Yd, Cd, c);
+    // coefficients of the point at time t into slot `v` (lead thread only)
+    auto coef = [&](double t, int v) {
+        if (lead) {
+            double Cd[MM::NCONST], c[NC];
 #pragma unroll
-        for (int q = 0; q < MM::NCOEF; ++q) cr[q] = (float)c[q];
+            for (int i = 0; i < MM::NCONST; ++i) Cd[i] = d.consts ? __ldg(d.consts + i) : 0.0;
+            MM::coef(t, Xd, Yd, Cd, c);
+#pragma unroll
+            for (int q = 0; q < MM::NCOEF; ++q) cs[(v * P + p) * NC + q] = (float)c[q];
+        }
     };
 
-    // stage input u = y + s k  ->  A (hi / lo TF32 parts)
-    auto write_stage = [&](float s, const float (&kre)[E], const float (&kim)[E]) {
+    // stage input u = y + s k -> A (hi / lo TF32 parts); populations -> rdiag[slot]
+    auto write_stage = [&](float s, const float (&kre)[E], const float (&kim)[E], int slot) {
         float hr[E], hi_[E], lr[E], li[E];
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             const float ur = fmaf(s, kre[e], yre[e]), ui = fmaf(s, kim[e], yim[e]);
-            hr[e] = gqtc::to_tf32(ur);
-            hi_[e] = gqtc::to_tf32(ui);
-            lr[e] = gqtc::to_tf32(ur - hr[e]);
-            li[e] = gqtc::to_tf32(ui - hi_[e]);
+            hr[e] = tf32_round(ur);
+            hi_[e] = tf32_round(ui);
+            lr[e] = tf32_round(ur - hr[e]);
+            li[e] = tf32_round(ui - hi_[e]);
+            if (n0 + e == j) rdiag[slot * P * N + p * N + j] = ur;
         }
         gqtc::tmem_st8(t_ahi + n0, hr);
         gqtc::tmem_st8(t_ahi + N + n0, hi_);
@@ -211,10 +237,10 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
 
     uint32_t phase = 0;
     // k = f(u) for the stage input in A; false when the MMA wait gave up (uniform over the CTA).
-    auto eval = [&](float (&kre)[E], float (&kim)[E]) -> bool {
+    auto eval = [&](float (&kre)[E], float (&kim)[E], int slot, int v) -> bool {
         gqtc::tmem_wait_st();
         gqtc::fence_before_sync();
-        __syncthreads();  // stage input complete in A; K buffer and rdiag free
+        __syncthreads();  // stage input complete in A; coefficients and populations written
         if (tid == 0) {
             gqtc::fence_after_sync();
 #pragma unroll
@@ -228,89 +254,76 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
             }
             gqtc::mma_commit(bar);
         }
+        float cq[T::NT];  // the point's coefficients of the operator terms (c_0 = 1)
+        cq[0] = 1.f;
+#pragma unroll
+        for (int q = 1; q < T::NT; ++q) cq[q] = cs[(v * P + p) * NC + (q - 1)];
         const bool ok = gqtc::mbar_wait_bounded(bar, phase, kMaxPolls);
         gqtc::fence_after_sync();
-        float Kr[E], Ki[E], ur[E], ui[E];
-        {
-            float a[8], b[8], c2[8], d2[8];
-            gqtc::tmem_ld8(t_d + 0 * N + n0, a);
-            gqtc::tmem_ld8(t_d + 1 * N + n0, b);
-            gqtc::tmem_ld8(t_ahi + n0, c2);
-            gqtc::tmem_ld8(t_ahi + N + n0, d2);
+        float Kr[E], Ki[E];
+#pragma unroll
+        for (int q = 0; q < T::NT; ++q) {
+            float a[8], b[8];
+            gqtc::tmem_ld8(t_d + (2 * q) * N + n0, a);
+            gqtc::tmem_ld8(t_d + (2 * q + 1) * N + n0, b);
             gqtc::tmem_wait_ld();
 #pragma unroll
             for (int e = 0; e < E; ++e) {
-                Kr[e] = a[e];
-                Ki[e] = b[e];
-                ur[e] = c2[e];
-                ui[e] = d2[e];
+                Kr[e] = (q == 0) ? a[e] : fmaf(cq[q], a[e], Kr[e]);
+                Ki[e] = (q == 0) ? b[e] : fmaf(cq[q], b[e], Ki[e]);
             }
+        }
+#pragma unroll
+        for (int e = 0; e < E; ++e) kbuf[(p * N + j) * LDK + n0 + e] = {Kr[e], Ki[e]};
+        float ur[E], ui[E];
+        if constexpr (MM::kWOffDiag) {  // element-wise jump terms off the diagonal need the stage input
+            float a[8], b[8], c2[8], d2[8];
+            gqtc::tmem_ld8(t_ahi + n0, a);
+            gqtc::tmem_ld8(t_ahi + N + n0, b);
             gqtc::tmem_ld8(t_alo + n0, c2);
             gqtc::tmem_ld8(t_alo + N + n0, d2);
             gqtc::tmem_wait_ld();
 #pragma unroll
             for (int e = 0; e < E; ++e) {
-                ur[e] += c2[e];
-                ui[e] += d2[e];
+                ur[e] = a[e] + c2[e];
+                ui[e] = b[e] + d2[e];
             }
         }
-#pragma unroll
-        for (int q = 0; q < MM::ND; ++q) {
-            float a[8], b[8];
-            gqtc::tmem_ld8(t_d + (2 * q + 2) * N + n0, a);
-            gqtc::tmem_ld8(t_d + (2 * q + 3) * N + n0, b);
-            gqtc::tmem_wait_ld();
-#pragma unroll
-            for (int e = 0; e < E; ++e) {
-                Kr[e] = fmaf(cr[q], a[e], Kr[e]);
-                Ki[e] = fmaf(cr[q], b[e], Ki[e]);
-            }
-        }
-        if constexpr (MM::NG > 0) {
-#pragma unroll
-            for (int e = 0; e < E; ++e) {
-                Cx<float> dv = {0.f, 0.f};
-#pragma unroll
-                for (int g = 0; g < MM::NG; ++g) {
-                    const Cx<float> v = ldc(MM::diag(g), n0 + e);
-                    dv.re = fmaf(cr[MM::ND + g], v.re, dv.re);
-                    dv.im = fmaf(cr[MM::ND + g], v.im, dv.im);
-                }
-                Kr[e] = fmaf(dv.re, ur[e], fmaf(-dv.im, ui[e], Kr[e]));
-                Ki[e] = fmaf(dv.re, ui[e], fmaf(dv.im, ur[e], Ki[e]));
-            }
-        }
-#pragma unroll
-        for (int e = 0; e < E; ++e) kbuf[(p * N + j) * LDK + n0 + e] = {Kr[e], Ki[e]};
-        if (j >= n0 && j < n0 + E) {
-#pragma unroll
-            for (int e = 0; e < E; ++e)
-                if (n0 + e == j) rdiag[p * N + j] = {ur[e], ui[e]};
-        }
-        const int give_up = __syncthreads_or(!ok);  // K and the diagonal complete
+        const int give_up = __syncthreads_or(!ok);  // K complete
         if (give_up) return false;
         phase ^= 1u;
 #pragma unroll
         for (int e = 0; e < E; ++e) {
-            const int n = n0 + e, el = n * N + j;
+            const int n = n0 + e;
             const Cx<float> kt = kbuf[(p * N + n) * LDK + j];  // K[j][n]
-            Cx<float> o = {Ki[e] + kt.im, kt.re - Kr[e]};       // -i (K[n][j] - conj(K[j][n]))
-            gqmatrix::cmac(o, ldc(MM::wjump(), el), Cx<float>{ur[e], ui[e]});
-            if constexpr (MM::NJ > 0) {
-                const int q1 = __ldg(MM::jbegin() + el + 1);
-                for (int q = __ldg(MM::jbegin() + el); q < q1; ++q) {
-                    Cx<float> w = ldc(MM::jcoef(), q);
-                    const int rate = __ldg(MM::jrate() + q);
-                    if (rate >= 0) {
-                        w.re *= cr[rate];
-                        w.im *= cr[rate];
-                    }
-                    const int a = __ldg(MM::jsrc() + q) / N;  // source rho_aa
-                    gqmatrix::cmac(o, w, rdiag[p * N + a]);
+            kre[e] = Ki[e] + kt.im;                             // -i (K[n][j] - conj(K[j][n]))
+            kim[e] = kt.re - Kr[e];
+            if constexpr (MM::kWOffDiag) {
+                if (n != j) {
+                    const Cx<float> w = ldc(MM::wjump(), n * N + j);
+                    kre[e] = fmaf(w.re, ur[e], fmaf(-w.im, ui[e], kre[e]));
+                    kim[e] = fmaf(w.re, ui[e], fmaf(w.im, ur[e], kim[e]));
                 }
             }
-            kre[e] = o.re;
-            kim[e] = o.im;
+        }
+        // jump terms of this thread: population rho_aa of the stage input into row e
+        for (int q = 0; q < jcount; ++q) {
+            const int idx = jl * MM::TCJ_MAX + q;
+            const int e = __ldg(MM::tcj_e() + idx);
+            const int rate = __ldg(MM::tcj_rate() + idx);
+            Cx<float> w = ldc(MM::tcj_coef(), idx);
+            if (rate >= 0) {
+                const float cr = cs[(v * P + p) * NC + rate];
+                w.re *= cr;
+                w.im *= cr;
+            }
+            const float x = rdiag[slot * P * N + p * N + __ldg(MM::tcj_a() + idx)];
+#pragma unroll
+            for (int ee = 0; ee < E; ++ee)
+                if (ee == e) {
+                    kre[ee] = fmaf(w.re, x, kre[ee]);
+                    kim[ee] = fmaf(w.im, x, kim[ee]);
+                }
         }
         return true;
     };
@@ -329,52 +342,60 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
         }
     };
 
+    // Evaluations it = 4 n + s (step n, stage s). Stage times: s = 0 at the previous step's end
+    // (t_in + 0 for n = 0), s = 1, 2 at t_mid = (n + 1/2) dt, s = 3 at t_mid + dt/2 - the times and
+    // roundings of gqfixed::RK4. Coefficients change at it = 0 and at s = 1, 3 (version cv).
     bool failed = false;
     {
         float kre[E], kim[E];
 #pragma unroll
         for (int e = 0; e < E; ++e) kre[e] = kim[e] = 0.f;
-        write_stage(0.f, kre, kim);
-        coef(d.t_in + 0.0);
-        for (int step = 0; step < d.num_steps && !failed; ++step) {
-            double t_mid = ((double)step + 0.5) * dt;
-            if (!eval(kre, kim)) { failed = true; break; }  // k1
-#pragma unroll
-            for (int e = 0; e < E; ++e) {
-                are[e] = kre[e];
-                aim[e] = kim[e];
+        int cv = 0;
+        coef(d.t_in + 0.0, cv);
+        write_stage(0.f, kre, kim, 0);
+        const int total = 4 * d.num_steps;
+        for (int it = 0; it < total; ++it) {
+            const int step = it >> 2, s = it & 3;
+            if (!eval(kre, kim, it & 1, cv)) {
+                failed = true;
+                break;
             }
-            write_stage(h2, kre, kim);
-            coef(d.t_in + t_mid);
-            if (!eval(kre, kim)) { failed = true; break; }  // k2
+            const int nslot = (it + 1) & 1;
+            if (s == 3) {
 #pragma unroll
-            for (int e = 0; e < E; ++e) {
-                are[e] = fmaf(2.f, kre[e], are[e]);
-                aim[e] = fmaf(2.f, kim[e], aim[e]);
-            }
-            write_stage(h2, kre, kim);
-            if (!eval(kre, kim)) { failed = true; break; }  // k3
-#pragma unroll
-            for (int e = 0; e < E; ++e) {
-                are[e] = fmaf(2.f, kre[e], are[e]);
-                aim[e] = fmaf(2.f, kim[e], aim[e]);
-            }
-            write_stage(h, kre, kim);
-            t_mid += dt2d;
-            coef(d.t_in + t_mid);
-            if (!eval(kre, kim)) { failed = true; break; }  // k4
-#pragma unroll
-            for (int e = 0; e < E; ++e) {
-                are[e] += kre[e];
-                aim[e] += kim[e];
-                F::accumulate(yre[e], cre[e], are[e], h6);
-                F::accumulate(yim[e], cim[e], aim[e], h6);
-            }
-            if (OUT == GQIS_OUT_MEAN && step >= d.warmup_steps) observe();
-            if (step + 1 < d.num_steps) {
+                for (int e = 0; e < E; ++e) {
+                    are[e] += kre[e];
+                    aim[e] += kim[e];
+                    F::accumulate(yre[e], cre[e], are[e], h6);
+                    F::accumulate(yim[e], cim[e], aim[e], h6);
+                }
+                if (OUT == GQIS_OUT_MEAN && step >= d.warmup_steps) observe();
+                if (step + 1 == d.num_steps) break;
 #pragma unroll
                 for (int e = 0; e < E; ++e) kre[e] = kim[e] = 0.f;
-                write_stage(0.f, kre, kim);  // input of the next step's k1
+                write_stage(0.f, kre, kim, nslot);  // input of the next step's k1 (same time)
+            } else {
+                const double t_mid = ((double)step + 0.5) * dt;
+                if (s == 0) {
+#pragma unroll
+                    for (int e = 0; e < E; ++e) {
+                        are[e] = kre[e];
+                        aim[e] = kim[e];
+                    }
+                    cv ^= 1;
+                    coef(d.t_in + t_mid, cv);
+                } else {
+#pragma unroll
+                    for (int e = 0; e < E; ++e) {
+                        are[e] = fmaf(2.f, kre[e], are[e]);
+                        aim[e] = fmaf(2.f, kim[e], aim[e]);
+                    }
+                    if (s == 2) {
+                        cv ^= 1;
+                        coef(d.t_in + (t_mid + dt2d), cv);
+                    }
+                }
+                write_stage(s == 2 ? h : h2, kre, kim, nslot);
             }
         }
     }
@@ -383,7 +404,7 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
     if (failed) {
         // the MMA of the last phase did not signal: wait once more (bounded), mark the tile's outputs
         gqtc::mbar_wait_bounded(bar, phase, kMaxPolls);
-        if (active && j == 0 && hh == 0) {
+        if (active && lead) {
             const int width = (OUT == GQIS_OUT_FINAL_STATE) ? MM::S : 2;
             for (int i = 0; i < width; ++i) out[(size_t)local * width + i] = __int_as_float(0x7fc00000);
         }
@@ -414,7 +435,7 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
             red[(1 * T::H + hh) * P + p] = osum_im;
         }
         __syncthreads();
-        if (j == 0 && hh == 0 && active) {
+        if (lead && active) {
             double sr = 0.0, si = 0.0;
             for (int g = 0; g < T::H; ++g) {
                 sr += red[(0 * T::H + g) * P + p];

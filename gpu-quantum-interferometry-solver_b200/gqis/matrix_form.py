@@ -304,7 +304,67 @@ def _interleave(z):
     return out
 
 
-def emit_matrix_model(mm: MatrixModel, form: str, uses_rho0_values: bool):
+def tensor_core_jump_lists(mm: MatrixModel, rows_per_thread=8):
+    """Jump terms of the tensor-core kernel grouped by thread: thread (column j, row block b)
+    owns rows b*8 .. b*8+7 of column j; each term is (row in block, source population a, coef,
+    rate index or -1). Element-wise terms on the diagonal become terms with a = own row.
+    Returns (lists[j][b], has_offdiagonal_elementwise)."""
+    Np = mm.Np
+    H = Np // rows_per_thread
+    lists = [[[] for _ in range(H)] for _ in range(Np)]
+    for dst, src, coef, rate in mm.jumps:
+        n, j = divmod(dst, Np)
+        a, b = divmod(src, Np)
+        if a != b:
+            raise ValueError("tensor-core jump lists need population sources")
+        lists[j][n // rows_per_thread].append((n % rows_per_thread, a, complex(coef), rate))
+    woff = False
+    for n in range(Np):
+        for j in range(Np):
+            w = complex(mm.wjump[n, j])
+            if w == 0:
+                continue
+            if n == j:
+                lists[j][n // rows_per_thread].append((n % rows_per_thread, n, w, -1))
+            else:
+                woff = True
+    return lists, woff
+
+
+def _tensor_core_tables(mm: MatrixModel):
+    lists, woff = tensor_core_jump_lists(mm)
+    Np = mm.Np
+    H = Np // 8
+    jmax = max(1, max(len(lists[j][b]) for j in range(Np) for b in range(H)))
+    count, e, a, coef, rate = [], [], [], [], []
+    for j in range(Np):
+        for b in range(H):
+            terms = lists[j][b] + [(0, 0, 0j, -1)] * (jmax - len(lists[j][b]))
+            count.append(len(lists[j][b]))
+            for (ee, aa, cc, rr) in terms:
+                e.append(ee)
+                a.append(aa)
+                coef.append(cc)
+                rate.append(rr)
+    arrays = [
+        _array("mm_tcj_count", "int", count),
+        _array("mm_tcj_e", "int", e),
+        _array("mm_tcj_a", "int", a),
+        _array("mm_tcj_rate", "int", rate),
+        _array("mm_tcj_coef", "mreal", _interleave(coef)),
+    ]
+    members = f"""    static constexpr int TCJ_MAX = {jmax};
+    static constexpr bool kWOffDiag = {'true' if woff else 'false'};
+    __device__ __forceinline__ static const int* tcj_count() {{ return mm_tcj_count; }}
+    __device__ __forceinline__ static const int* tcj_e() {{ return mm_tcj_e; }}
+    __device__ __forceinline__ static const int* tcj_a() {{ return mm_tcj_a; }}
+    __device__ __forceinline__ static const int* tcj_rate() {{ return mm_tcj_rate; }}
+    __device__ __forceinline__ static const mreal* tcj_coef() {{ return mm_tcj_coef; }}
+"""
+    return arrays, members
+
+
+def emit_matrix_model(mm: MatrixModel, form: str, uses_rho0_values: bool, tensor_cores=False):
     """C++ text of the model data and ``struct MM`` for ``csrc/gqis_matrix.cuh``.
 
     Operator data are printed with 17 significant digits in the form's type (``mreal``);
@@ -341,6 +401,10 @@ def emit_matrix_model(mm: MatrixModel, form: str, uses_rho0_values: bool):
     ]
     nconst = max(1, len(mm.runtime_const_syms))
     body = "\n".join("        " + ln for ln in coef_lines) or "        /* none */"
+    tc_members = ""
+    if tensor_cores:
+        tc_arrays, tc_members = _tensor_core_tables(mm)
+        parts += tc_arrays
     struct = f"""struct MM {{
     using real = mreal;
     static constexpr int N = {Np};
@@ -369,7 +433,7 @@ def emit_matrix_model(mm: MatrixModel, form: str, uses_rho0_values: bool):
     __device__ __forceinline__ static const mreal* jcoef() {{ return mm_jcoef; }}
     __device__ __forceinline__ static const double* obs_t() {{ return mm_obs_t; }}
     __device__ __forceinline__ static const double* rho0() {{ return mm_rho0; }}
-}};"""
+{tc_members}}};"""
     return "\n".join(parts + [struct])
 
 
@@ -384,10 +448,15 @@ def tensor_core_blockers(mm: MatrixModel, form: str):
         out.append("the tensor-core form is an FP32 form (precision='fp32')")
     if mm.Np not in TENSOR_DIMS:
         out.append(f"padded dimension {mm.Np} is not one of {TENSOR_DIMS}")
-    elif 2 * mm.Np * (1 + mm.num_dense) > 256:
-        out.append(f"{mm.num_dense} time-dependent operator terms exceed one MMA (2 N (1 + terms) <= 256)")
+    elif 2 * mm.Np * (1 + mm.num_dense + mm.num_diag) > 256:
+        out.append(f"{mm.num_dense + mm.num_diag} coefficient operator terms exceed one MMA "
+                   "(2 N (1 + terms) <= 256)")
     if any(src // mm.Np != src % mm.Np for _, src, _, _ in mm.jumps):
         out.append("a jump term reads an off-diagonal element (only populations may feed other elements)")
+    elif mm.Np in TENSOR_DIMS:
+        lists, _ = tensor_core_jump_lists(mm)
+        if max(len(x) for col in lists for x in col) > 32:
+            out.append("more than 32 jump terms land in one thread's eight rows")
     return out
 
 
@@ -400,7 +469,7 @@ def module_source(mm: MatrixModel, form: str, output_mode: str, uses_rho0_values
         blockers = tensor_core_blockers(mm, form)
         if blockers:
             raise ValueError("the tensor-core matrix form cannot run this model: " + "; ".join(blockers))
-    model = emit_matrix_model(mm, form, uses_rho0_values)
+    model = emit_matrix_model(mm, form, uses_rho0_values, tensor_cores)
     model_hash = int(hashlib.sha256(model.encode()).hexdigest()[:16], 16)
     form_type = {"fp64": "FormFP64", "fp32": "FormFP32"}[form]
     return "\n".join([
@@ -440,9 +509,9 @@ def flops_per_point_step(mm: MatrixModel):
 
 def tensor_flops_per_point_step(mm: MatrixModel):
     """Tensor-pipe arithmetic of one RK4 step of one point in the tcgen05 kernel: per RHS the
-    point's N rows of D (2 N (1 + ND) columns) over K = 2 N, three split-TF32 passes."""
+    point's N rows of D (2 N (1 + ND + NG) columns) over K = 2 N, three split-TF32 passes."""
     Np = mm.Np
-    return 4 * 3 * 2 * Np * (2 * Np * (1 + mm.num_dense)) * (2 * Np)
+    return 4 * 3 * 2 * Np * (2 * Np * (1 + mm.num_dense + mm.num_diag)) * (2 * Np)
 
 
 def dense_operators(mm: MatrixModel, X, Y, t, consts=()):
