@@ -19,12 +19,15 @@
 // compensated update, time and coefficients FP64, the mean of <O> FP64.
 //
 // Thread t: lane r = t % 128 (warp quadrant r / 32), rows n0 = 8 (t / 128) .. n0 + 7 of column j.
-// Coefficients are evaluated once per point and stage time by one thread and shared through
-// shared memory. Jump terms come from per-thread lists (the module's tcj_* tables) whose sources
-// are populations rho_aa, shared through shared memory when the stage input is written; element-
-// wise terms off the diagonal (kWOffDiag) read the stage input back from A (hi + lo).
-// Every mbarrier wait is bounded: on give-up the CTA writes NaN outputs, waits (bounded) for the
-// MMA in flight, frees its tensor memory and returns.
+// Diagonal operator terms go through the MMA (kDiagInMma, small N) or the epilogue (larger N,
+// where the MMA is the longer part of a stage). Coefficients are evaluated once per point and
+// stage time by one thread and shared through shared memory. Jump terms come from per-thread
+// lists (the module's tcj_* tables) whose sources are populations rho_aa, shared through shared
+// memory when the stage input is written; element-wise terms off the diagonal (kWOffDiag) and
+// diagonal terms done in the epilogue read the stage input back from A (hi + lo).
+// One thread polls the MMA's mbarrier (bounded); the CTA meets it at a barrier. On give-up the
+// CTA writes NaN outputs, waits (bounded) for the MMA in flight, frees its tensor memory and
+// returns.
 #pragma once
 
 #include <type_traits>
@@ -47,7 +50,8 @@ struct TcShape {
     static constexpr int H = N / E;           // threads per column
     static constexpr int THREADS = 128 * H;
     static constexpr int MIN_CTAS = 65536 / (THREADS * 128);  // keeps <= 128 registers per thread
-    static constexpr int NT = 1 + MM::ND + MM::NG;  // operator terms in B
+    static constexpr int NGM = MM::kDiagInMma ? MM::NG : 0;  // diagonal terms done by the MMA
+    static constexpr int NT = 1 + MM::ND + NGM;      // operator terms in B
     static constexpr int NMMA = 2 * N * NT;   // B / D columns
     static constexpr int KDIM = 2 * N;        // real-embedded inner dimension
     static constexpr int KCH = KDIM / 8;      // MMA K steps of 8 TF32
@@ -135,7 +139,7 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
         const int m = k % N;
         const bool imag_in = k >= N;
         float tr, ti;
-        if (q <= MM::ND) {
+        if (q <= MM::ND) {  // Heff0 and the dense terms; then the diagonal terms (NGM of them)
             const float* op = (q == 0) ? MM::heff() : MM::dense(q - 1);
             tr = __ldg(op + 2 * (n * N + m));
             ti = __ldg(op + 2 * (n * N + m) + 1);
@@ -225,8 +229,8 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
             const float ur = fmaf(s, kre[e], yre[e]), ui = fmaf(s, kim[e], yim[e]);
             hr[e] = tf32_round(ur);
             hi_[e] = tf32_round(ui);
-            lr[e] = tf32_round(ur - hr[e]);
-            li[e] = tf32_round(ui - hi_[e]);
+            lr[e] = ur - hr[e];  // |lo| <= 2^-11 |u|; its TF32 read loses at most 2^-21 |u|
+            li[e] = ui - hi_[e];
             if (n0 + e == j) rdiag[slot * P * N + p * N + j] = ur;
         }
         gqtc::tmem_st8(t_ahi + n0, hr);
@@ -258,7 +262,10 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
         cq[0] = 1.f;
 #pragma unroll
         for (int q = 1; q < T::NT; ++q) cq[q] = cs[(v * P + p) * NC + (q - 1)];
-        const bool ok = gqtc::mbar_wait_bounded(bar, phase, kMaxPolls);
+        // one thread polls the mbarrier; the others wait at the barrier instead of spinning
+        const bool ok = (tid != 0) || gqtc::mbar_wait_bounded(bar, phase, kMaxPolls);
+        if (__syncthreads_or(!ok)) return false;  // MMA complete (or given up, uniformly)
+        phase ^= 1u;
         gqtc::fence_after_sync();
         float Kr[E], Ki[E];
 #pragma unroll
@@ -273,10 +280,8 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
                 Ki[e] = (q == 0) ? b[e] : fmaf(cq[q], b[e], Ki[e]);
             }
         }
-#pragma unroll
-        for (int e = 0; e < E; ++e) kbuf[(p * N + j) * LDK + n0 + e] = {Kr[e], Ki[e]};
         float ur[E], ui[E];
-        if constexpr (MM::kWOffDiag) {  // element-wise jump terms off the diagonal need the stage input
+        if constexpr (MM::kWOffDiag || (T::NGM < MM::NG)) {  // terms that need the stage input itself
             float a[8], b[8], c2[8], d2[8];
             gqtc::tmem_ld8(t_ahi + n0, a);
             gqtc::tmem_ld8(t_ahi + N + n0, b);
@@ -289,9 +294,24 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
                 ui[e] = b[e] + d2[e];
             }
         }
-        const int give_up = __syncthreads_or(!ok);  // K complete
-        if (give_up) return false;
-        phase ^= 1u;
+        if constexpr (T::NGM < MM::NG) {  // diagonal terms in the epilogue: K += (sum_g c_g v_g[n]) u[n][j]
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                Cx<float> dv = {0.f, 0.f};
+#pragma unroll
+                for (int g = 0; g < MM::NG; ++g) {
+                    const Cx<float> vg = ldc(MM::diag(g), n0 + e);
+                    const float cg = cs[(v * P + p) * NC + MM::ND + g];
+                    dv.re = fmaf(cg, vg.re, dv.re);
+                    dv.im = fmaf(cg, vg.im, dv.im);
+                }
+                Kr[e] = fmaf(dv.re, ur[e], fmaf(-dv.im, ui[e], Kr[e]));
+                Ki[e] = fmaf(dv.re, ui[e], fmaf(dv.im, ur[e], Ki[e]));
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < E; ++e) kbuf[(p * N + j) * LDK + n0 + e] = {Kr[e], Ki[e]};
+        __syncthreads();  // K complete
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             const int n = n0 + e;
@@ -307,9 +327,9 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
             }
         }
         // jump terms of this thread: population rho_aa of the stage input into row e
+        float jre = 0.f, jim = 0.f;
         for (int q = 0; q < jcount; ++q) {
             const int idx = jl * MM::TCJ_MAX + q;
-            const int e = __ldg(MM::tcj_e() + idx);
             const int rate = __ldg(MM::tcj_rate() + idx);
             Cx<float> w = ldc(MM::tcj_coef(), idx);
             if (rate >= 0) {
@@ -318,11 +338,25 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
                 w.im *= cr;
             }
             const float x = rdiag[slot * P * N + p * N + __ldg(MM::tcj_a() + idx)];
+            if constexpr (MM::kJumpsOnDiagonal) {
+                jre = fmaf(w.re, x, jre);
+                jim = fmaf(w.im, x, jim);
+            } else {
+                const int e = __ldg(MM::tcj_e() + idx);
 #pragma unroll
-            for (int ee = 0; ee < E; ++ee)
-                if (ee == e) {
-                    kre[ee] = fmaf(w.re, x, kre[ee]);
-                    kim[ee] = fmaf(w.im, x, kim[ee]);
+                for (int ee = 0; ee < E; ++ee)
+                    if (ee == e) {
+                        kre[ee] = fmaf(w.re, x, kre[ee]);
+                        kim[ee] = fmaf(w.im, x, kim[ee]);
+                    }
+            }
+        }
+        if constexpr (MM::kJumpsOnDiagonal) {
+#pragma unroll
+            for (int e = 0; e < E; ++e)
+                if (n0 + e == j) {
+                    kre[e] += jre;
+                    kim[e] += jim;
                 }
         }
         return true;

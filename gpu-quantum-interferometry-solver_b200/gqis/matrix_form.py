@@ -331,6 +331,13 @@ def tensor_core_jump_lists(mm: MatrixModel, rows_per_thread=8):
     return lists, woff
 
 
+def diag_in_mma(mm: MatrixModel):
+    """Whether the tensor-core kernel multiplies the diagonal operator terms on the tensor cores
+    (one more MMA term per diagonal operator) or in its epilogue. Up to N = 16 the epilogue is
+    the longer part of a stage and the MMA has room; at N = 32 the MMA is the longer part."""
+    return mm.Np <= 16
+
+
 def _tensor_core_tables(mm: MatrixModel):
     lists, woff = tensor_core_jump_lists(mm)
     Np = mm.Np
@@ -353,8 +360,11 @@ def _tensor_core_tables(mm: MatrixModel):
         _array("mm_tcj_rate", "int", rate),
         _array("mm_tcj_coef", "mreal", _interleave(coef)),
     ]
+    on_diag = all(e + 8 * b == j for j in range(Np) for b in range(H) for (e, _, _, _) in lists[j][b])
     members = f"""    static constexpr int TCJ_MAX = {jmax};
     static constexpr bool kWOffDiag = {'true' if woff else 'false'};
+    static constexpr bool kJumpsOnDiagonal = {'true' if on_diag else 'false'};
+    static constexpr bool kDiagInMma = {'true' if diag_in_mma(mm) else 'false'};
     __device__ __forceinline__ static const int* tcj_count() {{ return mm_tcj_count; }}
     __device__ __forceinline__ static const int* tcj_e() {{ return mm_tcj_e; }}
     __device__ __forceinline__ static const int* tcj_a() {{ return mm_tcj_a; }}
@@ -448,7 +458,7 @@ def tensor_core_blockers(mm: MatrixModel, form: str):
         out.append("the tensor-core form is an FP32 form (precision='fp32')")
     if mm.Np not in TENSOR_DIMS:
         out.append(f"padded dimension {mm.Np} is not one of {TENSOR_DIMS}")
-    elif 2 * mm.Np * (1 + mm.num_dense + mm.num_diag) > 256:
+    elif 2 * mm.Np * (1 + mm.num_dense + (mm.num_diag if diag_in_mma(mm) else 0)) > 256:
         out.append(f"{mm.num_dense + mm.num_diag} coefficient operator terms exceed one MMA "
                    "(2 N (1 + terms) <= 256)")
     if any(src // mm.Np != src % mm.Np for _, src, _, _ in mm.jumps):
@@ -511,7 +521,8 @@ def tensor_flops_per_point_step(mm: MatrixModel):
     """Tensor-pipe arithmetic of one RK4 step of one point in the tcgen05 kernel: per RHS the
     point's N rows of D (2 N (1 + ND + NG) columns) over K = 2 N, three split-TF32 passes."""
     Np = mm.Np
-    return 4 * 3 * 2 * Np * (2 * Np * (1 + mm.num_dense + mm.num_diag)) * (2 * Np)
+    terms = 1 + mm.num_dense + (mm.num_diag if diag_in_mma(mm) else 0)
+    return 4 * 3 * 2 * Np * (2 * Np * terms) * (2 * Np)
 
 
 def dense_operators(mm: MatrixModel, X, Y, t, consts=()):
