@@ -475,7 +475,7 @@ def run_serving(args):
     from gqis.serving import SweepServer
     from test_support_calls import SERVING_SIDES, qubit_fit_model, serving_model
     rng = np.random.default_rng(args.seed)
-    dims = (2, 4, 8)
+    dims = (2, 4, 8, 16)
     reqs = []
     t = 0.0
     for _ in range(args.requests):
@@ -483,7 +483,9 @@ def run_serving(args):
         if rng.random() < 0.2:
             reqs.append((t, "fit", 256))
         else:
-            reqs.append((t, int(rng.choice(dims)), int(rng.choice(SERVING_SIDES))))
+            N = int(rng.choice(dims))
+            sides = SERVING_SIDES if N < 16 else tuple(x for x in SERVING_SIDES if x <= 512)
+            reqs.append((t, N, int(rng.choice(sides))))
     models = {}
     for _, N, side in reqs:
         if N != "fit" and (N, side) not in models:
@@ -545,12 +547,13 @@ def run_serving(args):
             errs.append(float(np.max(np.abs(g - fd)) / np.max(np.abs(fd))))
         fit_check = {"params": [str(p) for p in fit_params], "max_rel_err_vs_central_fd": errs}
     line = {
-        "metric": "sweep serving: aggregate points*steps/s and latency (Poisson 50/s, N in {2,4,8}, 20% fits)",
+        "metric": "sweep serving: aggregate points*steps/s and latency (Poisson 50/s, N in {2,4,8,16}, 20% fits)",
         "value": served, "unit": "points*steps/s", "n_gpus": 1, "steps": args.requests, "warmup": len(dims),
         "ms_per_step": float(np.mean(lat)), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"{args.requests} seeded requests, Poisson rate {args.rate}/s; 80% sweeps (N uniform "
-                               f"in {dims}, grid side uniform in {SERVING_SIDES}, mean <O> maps, RK4, FP32 form), "
+                               f"in {dims}, grid side uniform in {SERVING_SIDES} (N = 16: up to 512), mean <O> maps, RK4, "
+                               "FP32 form; N = 16 on the tensor-core density-matrix kernel), "
                                "20% fits (d<O>avg/d(Gamma1, Gamma_phi, Delta), 256x256 two-level map, 4000 RK4 "
                                "steps, checkpointed adjoint, FP64)",
                    "server": "4 streams, 32768-point chunks, <= 16 admitted requests, memory budget 50% free"},

@@ -411,7 +411,8 @@ def _solve_symbolic_system(H, Drive, Col_Ops, mean_operator, tlist,
     density-matrix kernel of ``matrix_form`` on the CUDA cores; fixed-step RK4, outputs
     ``mean``/``final``/``final_rho``, no time trace), ``"matrix_tc"`` (the same on the tensor
     cores, split-TF32 operands with FP32 accumulation; FP32 form, padded N of 8, 16 or 32) or
-    ``"auto"`` (matrix from N = 16 on where it applies).
+    ``"auto"`` (matrix from N = 16 on where it applies, on the tensor cores for FP32 sweeps the
+    tensor-core kernel can run).
     """
     if (calibrate_timesteps is not None and calibrate_timesteps is not False and not _prebuild_only
             and _prepare_only is None):
@@ -538,6 +539,8 @@ def _solve_symbolic_system(H, Drive, Col_Ops, mean_operator, tlist,
             H, Drive, Col_Ops, mean_operator, sweep_symbols=tuple(var_arrays), const_values=const_values,
             runtime_consts=runtime_consts, keep_symbolic_consts=keep_symbolic_consts,
             auto_runtime_consts=auto_runtime_consts, rho0=rho0, reuse=RHSreuse)
+        if rhs_form == "auto" and not matrix_form.tensor_core_blockers(compiled, form):
+            tensor_cores = True  # FP32 sweeps of N = 16 .. 32 run on the tensor cores
     elif compiled_rhs is None:
         compiled, rhs_status = _compile_rhs(
             H, Drive, Col_Ops, mean_operator, sweep_symbols=tuple(var_arrays), const_values=const_values,

@@ -7,7 +7,7 @@
 * the FP32 form against the same oracle: 2e-6 max-abs;
 * final_rho in the reduced layout, and rho0_values read back from it (a run split in two
   equals the run in one piece);
-* rhs_form="auto" picks the matrix form from N = 16 on;
+* rhs_form="auto" picks the matrix form from N = 16 on (tensor cores for FP32);
 * the tensor-core kernel (split-TF32 tcgen05 MMAs, FP32 accumulation and state) against the same
   oracle at N = 8, 16, 32: 5e-6 max-abs, and within 5e-6 of the CUDA-core FP32 form; final_rho
   through it as well. The grids leave the last tile of points partly empty.
@@ -81,6 +81,8 @@ def test_auto_picks_matrix_form_from_n16():
     import gqis
     w, args, kwargs = hilbert_model(16)
     _, info = gqis.mesolve_2D(*args, **kwargs, precision="fp32", return_timing_info=True)
+    assert info["rhs_form"] == "matrix_tc"
+    _, info = gqis.mesolve_2D(*args, **kwargs, precision="fp64", return_timing_info=True)
     assert info["rhs_form"] == "matrix"
 
 

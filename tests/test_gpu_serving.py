@@ -70,3 +70,17 @@ def test_fit_requests_in_the_server_match_the_adjoint_alone():
         f_sweep.result(300)
     np.testing.assert_array_equal(out["result"], mean)
     np.testing.assert_array_equal(out["grad"], grad)
+
+
+@pytest.mark.gpu
+def test_tensor_core_request_is_the_same_in_chunks_that_split_tiles():
+    """The tensor-core kernel packs 128 / N points per MMA tile; a chunk size that is not a multiple
+    of the tile moves every point to another row of another tile, and the result must not change."""
+    import gqis
+    from gqis.serving import SweepServer
+    from test_support_calls import hilbert_model
+    _, args, kwargs = hilbert_model(16, side=(12, 9))
+    alone = gqis.mesolve_2D(*args, **kwargs, precision="fp32", rhs_form="matrix_tc")
+    with SweepServer(streams=3, chunk_points=13, max_inflight=4) as srv:
+        out = srv.submit("mesolve_2D", *args, **kwargs, precision="fp32", rhs_form="matrix_tc").result(300)
+    np.testing.assert_array_equal(out["result"], alone)
