@@ -393,7 +393,8 @@ def run_hilbert(args):
     sys.path.insert(0, str(ROOT / "oracle"))
     import lindblad_oracle
     from gqis import native, solver, workloads
-    peaks = {"fp64": native.probe_fma_tflops(0), "fp32": native.probe_fma_tflops(1)}
+    peaks = {"fp64": native.probe_fma_tflops(0), "fp32": native.probe_fma_tflops(1),
+             "tf32_tensor": native.probe_tc_tf32_tflops()}
     dims = tuple(int(n) for n in args.dims.split(","))
     flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
     rows = {}
@@ -422,6 +423,7 @@ def run_hilbert(args):
             if rhs_form == "matrix_tc":
                 tf = sweep.launch_spec.entry["frag"]["tensor_flops_per_point_step"] * points * steps
                 row[f"{rhs_form}_{prec}"]["tensor_pipe_tflops"] = tf / (ms / 1e3) / 1e12
+                row[f"{rhs_form}_{prec}"]["frac_of_measured_tf32_tensor_peak"] = tf / (ms / 1e3) / 1e12 / peaks["tf32_tensor"]
             del sweep
         # the FP64 oracle on 4 points of the grid (full 2000 steps)
         eps, A = w["symbols"]
@@ -456,6 +458,11 @@ def run_hilbert(args):
                                f"{args.hsteps} RK4 steps of dt 0.05, mean <|N-1><N-1|>", "dims": list(dims),
                    "l2": "flushed (256 MiB write) between timed launches"},
         "per_dimension": {str(k): v for k, v in rows.items()},
+        "roofline": ({"bound": "tensor", "achieved": head[hk]["tensor_pipe_tflops"], "peak": peaks["tf32_tensor"],
+                      "unit": "TFLOP/s", "frac": head[hk]["tensor_pipe_tflops"] / peaks["tf32_tensor"],
+                      "traffic": None, "peak_source": "tcgen05 kind::tf32 probe (gqis_probe_tc_tf32), same run",
+                      "kernel": f"matrix_tc_kernel N={16 if 16 in rows else dims[0]}"}
+                     if hk == "matrix_tc_fp32" else None),
         "measured_fma_peaks_tflops": peaks, "clocks": clocks,
     }
     print(json.dumps(line))

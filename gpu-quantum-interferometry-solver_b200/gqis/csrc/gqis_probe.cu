@@ -1,4 +1,5 @@
-// gqis_probe.cu - CUDA-core FMA throughput probes (FP64 DFMA, FP32 FFMA, packed FP32 FFMA2).
+// gqis_probe.cu - throughput probes: CUDA-core FMA (FP64 DFMA, FP32 FFMA, packed FP32 FFMA2) and
+// the tcgen05 tensor-core MMA of kind::tf32 (the instruction of the tensor-core density-matrix kernel).
 //
 // The sweep kernels are bound by the FP32 / FP64 FMA pipes, which have no entry in the
 // measured-peaks file of this machine; these probes measure them on the device that runs the
@@ -9,6 +10,7 @@
 #include <stdint.h>
 
 #include "gqis_b200.h"
+#include "gqis_tcgen05.cuh"
 
 namespace {
 
@@ -61,9 +63,117 @@ __global__ void __launch_bounds__(kBlock) fma32x2_kernel(int iters, float* out) 
     if (s == 123.456f) out[blockIdx.x] = s;
 }
 
+// ---- tcgen05 kind::tf32: one CTA per SM issues `iters` x 4 MMAs of M = 128, N = 256, K = 8 (A in
+// tensor memory, B in shared memory, as the density-matrix kernel does) back to back and waits once.
+constexpr int kTcN = 256, kTcKSteps = 4;
+constexpr size_t kTcSmem = 120 * 1024;  // > half of the SM's shared memory: one CTA per SM
+
+__global__ void __launch_bounds__(128, 1) tc_tf32_kernel(int iters, float* out, int* status) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    float* b = reinterpret_cast<float*>(smem);  // kTcKSteps x 256 rows x 8 TF32, K-major
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kTcKSteps * kTcN * 32);
+    uint32_t* slot = reinterpret_cast<uint32_t*>(smem + kTcKSteps * kTcN * 32 + 8);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    for (int e = tid; e < kTcKSteps * kTcN * 8; e += blockDim.x) b[e] = (float)((e % 7) - 3) * 0.125f;
+    gqtc::fence_proxy_async_smem();
+    if (tid == 0) gqtc::mbar_init(bar, 1);
+    if (warp == 0) {
+        gqtc::tmem_alloc(slot, 512);
+        gqtc::tmem_relinquish();
+    }
+    gqtc::fence_before_sync();
+    __syncthreads();
+    gqtc::fence_after_sync();
+    const uint32_t tbase = *slot;
+    const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
+    float v[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) v[i] = (float)((tid + i) % 5) * 0.25f;
+#pragma unroll
+    for (int kc = 0; kc < kTcKSteps; ++kc) gqtc::tmem_st8(tbase + lane_base + kTcN + 8 * kc, v);
+    gqtc::tmem_wait_st();
+    gqtc::fence_before_sync();
+    __syncthreads();
+    bool ok = true;
+    if (tid == 0) {
+        gqtc::fence_after_sync();
+        const uint32_t idesc = gqtc::idesc_tf32_m128(kTcN);
+        const uint32_t baddr = gqtc::smem_u32(b);
+        for (int it = 0; it < iters; ++it) {
+#pragma unroll
+            for (int kc = 0; kc < kTcKSteps; ++kc)
+                gqtc::mma_tf32_ts(tbase, tbase + kTcN + 8 * kc, gqtc::smem_desc_kmajor(baddr + kc * kTcN * 32, 128, 256),
+                                  idesc, (it | kc) ? 1u : 0u);
+        }
+        gqtc::mma_commit(bar);
+        ok = gqtc::mbar_wait_bounded(bar, 0, 1u << 26);
+        if (!ok) atomicExch(status, 1);
+    }
+    __syncthreads();
+    gqtc::fence_after_sync();
+    float d[8];
+    gqtc::tmem_ld8(tbase + lane_base, d);
+    gqtc::tmem_wait_ld();
+    if (d[0] == 123.456f) out[blockIdx.x] = d[1];  // keeps the result alive, never true in practice
+    gqtc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        gqtc::fence_after_sync();
+        gqtc::tmem_dealloc(tbase, 512);
+    }
+}
+
 }  // namespace
 
 extern "C" {
+
+// Measured dense TF32 tensor-core rate (best of `repeats` launches after a warm-up) in 1e12 flop/s.
+// Returns GQIS_ERR_CUDA if an MMA chain did not signal completion within its bounded wait.
+__attribute__((visibility("default"))) int gqis_probe_tc_tf32(int iters, int repeats, double* tflops) {
+    if (!tflops || iters < 1 || repeats < 1) return GQIS_ERR_INVALID;
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return GQIS_ERR_CUDA;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return GQIS_ERR_CUDA;
+    if (cudaFuncSetAttribute(tc_tf32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem) != cudaSuccess)
+        return GQIS_ERR_CUDA;
+    void* out = nullptr;
+    int* status = nullptr;
+    if (cudaMalloc(&out, sizeof(float) * sms) != cudaSuccess) return GQIS_ERR_CUDA;
+    if (cudaMalloc(&status, sizeof(int)) != cudaSuccess) {
+        cudaFree(out);
+        return GQIS_ERR_CUDA;
+    }
+    cudaMemset(status, 0, sizeof(int));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    double best = 0.0;
+    int rc = GQIS_OK;
+    for (int r = 0; r <= repeats; ++r) {
+        cudaEventRecord(e0);
+        tc_tf32_kernel<<<sms, 128, kTcSmem>>>(iters, (float*)out, status);
+        cudaEventRecord(e1);
+        if (cudaEventSynchronize(e1) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+            rc = GQIS_ERR_CUDA;
+            break;
+        }
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        const double flops = 2.0 * 128.0 * kTcN * 8.0 * kTcKSteps * (double)iters * sms;
+        if (r > 0 && ms > 0.0f) best = fmax(best, flops / (ms * 1e-3) / 1e12);
+    }
+    int host_status = 0;
+    if (rc == GQIS_OK && cudaMemcpy(&host_status, status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+        rc = GQIS_ERR_CUDA;
+    if (rc == GQIS_OK && host_status != 0) rc = GQIS_ERR_CUDA;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    cudaFree(status);
+    *tflops = best;
+    return rc;
+}
+
 
 // kind: 0 = FP64 DFMA, 1 = FP32 FFMA, 2 = packed FP32 FFMA2. On success *tflops holds the
 // measured rate (best of `repeats` launches) in 1e12 flop/s.

@@ -1,6 +1,6 @@
 """The package's fixed native libraries (built in-tree by nvcc for sm_100a).
 
-* ``libgqis_probe.so``  - FMA-pipe throughput probes (roofline denominators);
+* ``libgqis_probe.so``  - FMA-pipe and TF32 tensor-core throughput probes (roofline denominators);
 * ``libgqis_serve.so``  - the continuous-batching sweep server (C++ host runtime).
 
 Model modules (one per model variant) are built separately by ``engine``.
@@ -73,4 +73,16 @@ def probe_fma_tflops(kind, iters=4096, repeats=3):
     rc = lib.gqis_probe_fma(int(kind), int(iters), int(repeats), ctypes.byref(out))
     if rc != 0:
         raise RuntimeError(f"gqis_probe_fma failed with status {rc}")
+    return out.value
+
+
+def probe_tc_tf32_tflops(iters=4096, repeats=3):
+    """Measured dense TF32 tensor-core rate in TFLOP/s (tcgen05 kind::tf32, M=128, N=256, K=8)."""
+    lib = load("gqis_probe")
+    lib.gqis_probe_tc_tf32.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    lib.gqis_probe_tc_tf32.restype = ctypes.c_int
+    out = ctypes.c_double()
+    rc = lib.gqis_probe_tc_tf32(int(iters), int(repeats), ctypes.byref(out))
+    if rc != 0:
+        raise RuntimeError(f"gqis_probe_tc_tf32 failed with status {rc}")
     return out.value
