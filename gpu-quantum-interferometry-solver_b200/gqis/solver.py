@@ -51,6 +51,7 @@ TIMESTEP_CALIBRATION_DEFAULTS = {
     "reset": False,
     "on_fail": "warning",
     "range_warning": True,
+    "batch_levels": 1,
 }
 _CALIBRATION_MAX_HALVINGS = 6
 TIMESTEP_CALIBRATION_ODE_DEFAULTS = {"rms_atol": 1e-4, "max_atol": 1e-3}
@@ -184,6 +185,45 @@ def _device_buffers(launch: SweepLaunch, point_begin=0, point_count=None):
     tensors = {"par_x": px, "par_y": py, "consts": consts, "rho0": rho0, "results": results,
                "trace": trace, "step_counts": counts, "work_counter": counter}
     return desc, tensors
+
+
+def _device_run_many(launches):
+    """Launch several sweeps at once, each on its own stream, and wait for all of them.
+
+    Used by the batched calibration search: its candidate resolutions are small launches whose
+    results are only needed together. Returns ``[(results, trace, step_counts, 0.0), ...]``.
+    """
+    torch = _torch()
+    done = []
+    current = torch.cuda.current_stream()
+    for launch in launches:
+        module = _load_kernel(launch.entry)
+        desc, buf = _device_buffers(launch)
+        stream = torch.cuda.Stream()
+        stream.wait_stream(current)  # inputs were uploaded on the current stream
+        module.launch(desc, stream.cuda_stream)
+        done.append(buf)
+    torch.cuda.synchronize()
+    return [(b["results"], b["trace"], b["step_counts"], 0.0) for b in done]
+
+
+def _with_steps(launch, steps, duration, warmup_time):
+    """The fixed-step launch ``launch`` with ``steps`` uniform steps over ``duration``."""
+    import dataclasses
+    warmup_time = float(warmup_time or 0.0)
+    warm = steps if warmup_time >= 1.0 else int(np.floor(warmup_time * steps))
+    return dataclasses.replace(launch, num_steps=int(steps), dt=float(duration) / steps,
+                               warmup_steps=max(0, min(int(steps), warm)))
+
+
+def _calibration_map(launch, results):
+    """Device results of one calibration launch as the map ``mesolve_2D`` would return."""
+    res = results.cpu().numpy() if hasattr(results, "cpu") else np.asarray(results)
+    nx, ny = len(launch.par_x), len(launch.par_y)
+    if launch.output_mode in ("mean", "final"):
+        out = (res[:, 0] + 1j * res[:, 1]).reshape(nx, ny)
+        return out.astype(np.complex128 if launch.form == "fp64" else np.complex64, copy=False)
+    return res.reshape(nx, ny, launch.state_size)
 
 
 def _device_run(launch: SweepLaunch):
@@ -879,6 +919,12 @@ def _calibrate_timestep(args, settings, base_steps, duration):
     Fixed-step solvers refine the step count by 2 (Richardson estimate with the method order,
     order 1 for mean outputs); adaptive solvers refine 1/tolerance by 10 (error ~ tolerance).
     A passing bracket is narrowed by ``bisection_steps`` geometric bisections.
+
+    Candidates of a fixed-step search are launched from one prepared launch of the test grid with
+    only the step count changed (no front-end pass per candidate). ``batch_levels`` > 1 runs the
+    next refinements (and later the next coarsenings) together, each candidate on its own stream with
+    one synchronisation; the candidates are then checked in the order of the one-at-a-time search, so
+    the outcome is the same. Speculative candidates beyond the accepted one cost device time.
     """
     start = time.time()
     test, full_grid = _undersampled_arguments(args, settings["sample_stride"])
@@ -898,16 +944,51 @@ def _calibrate_timestep(args, settings, base_steps, duration):
         return x / factor if adaptive else x // 2
 
     stored = {}
+    batch = max(1, int(settings.get("batch_levels", 1)))
+    results = {}
+    template = []  # a prepared launch of the test grid (fixed-step candidates differ only in steps)
+
+    def candidate(x):
+        t = dict(test)
+        if adaptive:
+            t["adaptive_options"] = _scaled_adaptive_options(args, value(x))
+        else:
+            t["tlist"] = np.linspace(0.0, duration, x + 1)
+        return t
+
+    def run_batch(xs):
+        xs = [x for x in dict.fromkeys(xs) if x not in results]
+        pending = []
+        for x in xs:
+            if template and not adaptive:  # only the step count differs: no front-end pass
+                pending.append((x, _with_steps(template[0], x, duration, args.get("warmup_time", 0.0))))
+                continue
+            holder = {}
+            ret = _solve_symbolic_system(**dict(candidate(x), _prepare_only=holder))
+            if "launch" in holder:
+                pending.append((x, holder["launch"]))
+                template.append(holder["launch"])
+            else:  # a solver stand-in that computes directly
+                results[x] = np.asarray(ret)
+        outs = _device_run_many([launch for _, launch in pending]) if pending else []
+        for (x, launch), out in zip(pending, outs):
+            results[x] = _calibration_map(launch, out[0])
+        if full_grid:
+            for x in xs:
+                stored[value(x)] = results[x]
 
     def run(x):
-        if adaptive:
-            test["adaptive_options"] = _scaled_adaptive_options(args, value(x))
-        else:
-            test["tlist"] = np.linspace(0.0, duration, x + 1)
-        r = np.asarray(_solve_symbolic_system(**test))
-        if full_grid:
-            stored[value(x)] = r
-        return r
+        run_batch([x])
+        return results[x]
+
+    def refinements(x):  # x refined `batch` times, as the search would step through them
+        out, c = [], x
+        for _ in range(batch):
+            c = factor * c
+            if c > x_limit:
+                break
+            out.append(c)
+        return out
 
     def check(x, coarse, fine_x, fine):
         rec = {label: value(x), "rms": np.inf, "max": np.inf}
@@ -923,14 +1004,17 @@ def _calibrate_timestep(args, settings, base_steps, duration):
               and (not settings["check_max"] or rec["max"] <= max_lim))
         return rec, ok
 
-    x, coarse = base, run(base)
+    run_batch([base] + refinements(base)[:batch - 1])
+    x, coarse = base, results[base]
     tested, status, accepted = [], None, None
     ref_x = ref = None
     while status is None:
         if factor * x > x_limit:
             status, accepted = ("min_step_tol" if adaptive else "max_steps"), x
             break
-        fine = run(factor * x)
+        if factor * x not in results:
+            run_batch(refinements(x))
+        fine = results[factor * x]
         if adaptive and np.all(np.isfinite(coarse)) and not np.all(np.isfinite(fine)):
             status, accepted = "max_substeps", x
             break
@@ -956,6 +1040,14 @@ def _calibrate_timestep(args, settings, base_steps, duration):
         while failing is None and (adaptive or accepted >= 2) and halvings < _CALIBRATION_MAX_HALVINGS:
             halvings += 1
             cand = coarser(accepted)
+            if cand not in results and batch > 1:  # the next coarsenings, as the loop would try them
+                seq, c = [], accepted
+                for _ in range(min(batch, _CALIBRATION_MAX_HALVINGS - halvings + 1)):
+                    if not (adaptive or c >= 2):
+                        break
+                    c = coarser(c)
+                    seq.append(c)
+                run_batch(seq)
             if passes(cand):
                 accepted = cand
             else:

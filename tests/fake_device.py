@@ -44,6 +44,10 @@ class FakeDevice:
         return res, trace, counts, 0.0
 
 
+    def device_run_many(self, launches):
+        return [self.device_run(launch) for launch in launches]
+
+
 def clear_caches():
     for cache in (_RHS_CODE_CACHE, core._KERNEL_CACHE, core._TIMESTEP_CALIBRATION_CACHE):
         cache.clear()
@@ -54,7 +58,8 @@ def fake_device(values=None):
     dev = FakeDevice(values)
     clear_caches()
     with patch.dict("os.environ", {"GQIS_DISK_CACHE": "0"}), \
-            patch.object(core, "_load_kernel", dev.load_kernel), patch.object(core, "_device_run", dev.device_run):
+            patch.object(core, "_load_kernel", dev.load_kernel), patch.object(core, "_device_run", dev.device_run), \
+            patch.object(core, "_device_run_many", dev.device_run_many):
         try:
             yield dev
         finally:
