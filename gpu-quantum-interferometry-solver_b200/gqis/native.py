@@ -1,7 +1,7 @@
 """The package's fixed native libraries (built in-tree by nvcc for sm_100a).
 
 * ``libgqis_probe.so``  - FMA-pipe and TF32 tensor-core throughput probes (roofline denominators);
-* ``libgqis_serve.so``  - the continuous-batching sweep server (C++ host runtime).
+* ``libgqis_render.so`` - phase-space rasteriser kernels (``gqis.render``).
 
 Model modules (one per model variant) are built separately by ``engine``.
 """
@@ -16,7 +16,7 @@ from pathlib import Path
 from .engine import ARCH_FLAGS, CSRC_DIR, INCLUDE_DIR, PACKAGE_DIR, nvcc_path
 
 BUILD_DIR = PACKAGE_DIR / "_build"
-LIBS = {"gqis_probe": ["gqis_probe.cu"], "gqis_serve": ["gqis_serve.cu"]}
+LIBS = {"gqis_probe": ["gqis_probe.cu"], "gqis_render": ["gqis_render.cu"]}
 _loaded: dict = {}
 
 

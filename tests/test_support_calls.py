@@ -80,6 +80,9 @@ def calls():
         for extra in ({}, {"nvrtc_options": ("-DGQ_STATIC_SCHEDULE=1",)}):
             _, args, kwargs = duffing_case(solver=solver, **extra)
             out.append(("odesolve_2D", args, kwargs))
+    _, args, kwargs = duffing_case(side=16, solver="rk4")  # state trace binned by the rasteriser tests
+    kwargs.pop("adaptive_options")
+    out.append(("odesolve_2D", args, kwargs))
     return out
 
 
