@@ -209,6 +209,11 @@ struct PointCtx {
         M::template drives<F>(Xd, Yd, t_abs, X, Y, Dr, Sd, Sr, Cd, Cr);
     }
 
+    // drives with the model's functions of time alone (M::time_funcs at t_abs) given in Tf
+    __device__ __forceinline__ void drives_tf(double t_abs, const double* Tf, R* Dr) const {
+        M::template drives_tf<F>(Xd, Yd, t_abs, X, Y, Dr, Sd, Sr, Cd, Cr, Tf);
+    }
+
     __device__ __forceinline__ void rhs(const R* y, const R* Dr, R* dy) const {
         M::rhs(y, X, Y, Dr, Sr, dy, Cr);
     }

@@ -18,6 +18,21 @@ namespace gqfixed {
 // compensated FP32 update (running correction c, h applied as hi + lo) in the FP32 form.
 
 // ------------------------------------------------------------------- classical RK4
+// Functions of time alone at the stage times of steps step .. step + kTimes/2 - 1 (entry 2s: the
+// step's midpoint, entry 2s + 1: its end, computed as in RK4::run), entries split over the warp's
+// lanes. Not inlined: its FP64 transcendental code would otherwise raise the register count of
+// the whole integration loop; it runs once per kTimes/2 steps.
+template <class M, int kTimes>
+__device__ __noinline__ void fill_time_table(const gqis_sweep_desc& d, int step, int rank, int nlanes,
+                                             const double* Cd, double* tab) {
+    const double dt = d.dt, dt2d = dt * 0.5;
+    for (int e = rank; e < kTimes; e += nlanes) {
+        double te = ((double)(step + (e >> 1)) + 0.5) * dt;
+        if (e & 1) te += dt2d;
+        M::time_funcs(d.t_in + te, Cd, tab + e * M::NTF);
+    }
+}
+
 struct RK4 {
     template <class M, class F, int OUT, int TRACE>
     __device__ __forceinline__ static void run(const gqis_sweep_desc& d, int64_t local, int64_t p) {
@@ -36,11 +51,32 @@ struct RK4 {
         const double dt2d = dt * 0.5;
         const R h = (R)dt, h2 = (R)dt2d;
         const Coef<R> h6 = Coef<R>::make(dt / 6.0);
+        // Functions of time alone (M::NTF of them) are the same for every point: each warp evaluates
+        // them for the stage times of kChunk steps at once into shared memory (lanes of the warp past
+        // the end of the grid have exited, so the warp synchronises only its remaining lanes).
+        constexpr int kChunk = 16, kTimes = 2 * kChunk;
+        constexpr int NTF = M::NTF;
+        __shared__ double tf_table[NTF > 0 ? GQ_BLOCK / 32 : 1][NTF > 0 ? kTimes * NTF : 1];
+        double* const tab = tf_table[NTF > 0 ? (threadIdx.x >> 5) : 0];
+        const int lane = threadIdx.x & 31;
+        const int64_t valid = d.point_count - (local - lane);  // lanes of this warp inside the grid
+        const unsigned warp_mask = valid >= 32 ? 0xffffffffu : ((1u << valid) - 1u);
+        const int rank = __popc(warp_mask & ((1u << lane) - 1u)), nlanes = __popc(warp_mask);
         pc.drives(d.t_in + 0.0, Dr);
         pc.rhs(y, Dr, k);
         for (int step = 0; step < d.num_steps; ++step) {
             double t_mid = ((double)step + 0.5) * dt;
-            pc.drives(d.t_in + t_mid, Dr);
+            const int slot = step % kChunk;
+            if constexpr (NTF > 0) {
+                if (slot == 0) {
+                    __syncwarp(warp_mask);  // the previous chunk is consumed
+                    fill_time_table<M, kTimes>(d, step, rank, nlanes, pc.Cd, tab);
+                    __syncwarp(warp_mask);
+                }
+                pc.drives_tf(d.t_in + t_mid, tab + (2 * slot) * NTF, Dr);
+            } else {
+                pc.drives(d.t_in + t_mid, Dr);
+            }
 #pragma unroll
             for (int i = 0; i < S; ++i) {
                 yt[i] = fma(h2, k[i], y[i]);
@@ -54,7 +90,11 @@ struct RK4 {
             }
             pc.rhs(yt, Dr, k);
             t_mid += dt2d;
-            pc.drives(d.t_in + t_mid, Dr);
+            if constexpr (NTF > 0) {
+                pc.drives_tf(d.t_in + t_mid, tab + (2 * slot + 1) * NTF, Dr);
+            } else {
+                pc.drives(d.t_in + t_mid, Dr);
+            }
 #pragma unroll
             for (int i = 0; i < S; ++i) {
                 yt[i] = fma(h, k[i], y[i]);

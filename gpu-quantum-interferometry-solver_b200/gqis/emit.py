@@ -155,8 +155,24 @@ def emit_model(compiled, uses_rho0_values):
     n_static = 0
     n_drive = len(drive_syms)
 
-    drive_lines += [f"const double {s} = {ccode(f, cast=False, phased=True)};" for s, f in func_temps]
-    drive_lines += [f"Drive_arr[{k}] = {ccode(e, cast=False, phased=True)};"
+    # Functions of time alone (cos(w t), with runtime constants at most) are the same for every
+    # point: they become Tf[k], which the RK4 kernel evaluates once per warp for a block of steps.
+    uniform = {str(x) for x in plan.get("runtime_const_syms", ())} | {"t"}
+    time_funcs = {}
+
+    def factor_time(e):
+        found = {}
+        walk = sp.preorder_traversal(sp.sympify(e))
+        for sub in walk:
+            if isinstance(sub, sp.Function) and sub.free_symbols \
+                    and {str(x) for x in sub.free_symbols} <= uniform and "t" in {str(x) for x in sub.free_symbols}:
+                k = time_funcs.setdefault(sub, len(time_funcs))
+                found[sub] = sp.Symbol(f"GQTF{k}")
+                walk.skip()
+        return sp.sympify(e).xreplace(found) if found else e
+
+    drive_lines += [f"const double {s} = {ccode(factor_time(f), cast=False, phased=True)};" for s, f in func_temps]
+    drive_lines += [f"Drive_arr[{k}] = {ccode(factor_time(e), cast=False, phased=True)};"
                     for k, e in enumerate(drive_exprs)]
 
     def bind(s, e, level):
@@ -167,7 +183,7 @@ def emit_model(compiled, uses_rho0_values):
             names[str(s)] = f"Static_arr[{n_static}]"
             n_static += 1
         else:
-            line = f"Drive_arr[{n_drive}] = {ccode(e, cast=False, phased=True)};"
+            line = f"Drive_arr[{n_drive}] = {ccode(factor_time(e), cast=False, phased=True)};"
             drive_lines.append(_substitute(line, list(names.items())))
             names[str(s)] = f"Drive_arr[{n_drive}]"
             n_drive += 1
@@ -217,19 +233,31 @@ def emit_model(compiled, uses_rho0_values):
 
     static_lines = finish(static_lines, False)
     drive_lines = [_fp64_names(ln) for ln in finish(drive_lines, False)]
+    tf_names = [(f"GQTF{k}", f"Tf[{k}]") for k in range(len(time_funcs))]
+    drive_lines = [_substitute(ln, tf_names) for ln in drive_lines]
+    funcs = sorted(time_funcs, key=time_funcs.get)
+    time_inline = [_fp64_names(ln) for ln in finish([f"Tf[{k}] = {ccode(f, cast=False, phased=True)};"
+                                                     for k, f in enumerate(funcs)], False)]
+    time_exact = [_fp64_names(ln) for ln in finish(
+        [f"Tf[{k}] = {ccode(f, cast=False)};" for k, f in enumerate(funcs)], False)]
     rhs_lines = finish(rhs_lines, True)
     init_lines = finish(init_lines, False)
     obs_re, obs_im = finish([obs_re, obs_im], True)
 
-    used = sorted({int(m) for part in (static_lines, drive_lines, rhs_lines, init_lines, [obs_re, obs_im])
-                   for line in part for m in re.findall(r"Const_arr\[(\d+)\]", line)})
+    # drive and time lines read the FP64 copies (Const_d), the others Const_arr: both count and both
+    # are renumbered
+    used = sorted({int(m) for part in (static_lines, drive_lines, rhs_lines, init_lines, [obs_re, obs_im],
+                                       time_inline, time_exact)
+                   for line in part for m in re.findall(r"Const_(?:arr|d)\[(\d+)\]", line)})
     if used and used != list(range(len(plan["runtime_const_syms"]))):
         remap = {old: new for new, old in enumerate(used)}
 
         def renumber(line):
-            return re.sub(r"Const_arr\[(\d+)\]", lambda m: f"Const_arr[{remap[int(m.group(1))]}]", line)
-        static_lines, drive_lines, rhs_lines, init_lines = (
-            [renumber(x) for x in part] for part in (static_lines, drive_lines, rhs_lines, init_lines))
+            return re.sub(r"Const_(arr|d)\[(\d+)\]",
+                          lambda m: f"Const_{m.group(1)}[{remap[int(m.group(2))]}]", line)
+        static_lines, drive_lines, rhs_lines, init_lines, time_inline, time_exact = (
+            [renumber(x) for x in part]
+            for part in (static_lines, drive_lines, rhs_lines, init_lines, time_inline, time_exact))
         obs_re, obs_im = renumber(obs_re), renumber(obs_im)
 
     return {"state_size": size, "n_static": max(1, n_static), "n_drive": max(1, n_drive),
@@ -238,6 +266,8 @@ def emit_model(compiled, uses_rho0_values):
             "static_lines": tuple(static_lines), "drive_lines": tuple(drive_lines),
             "rhs_lines": tuple(rhs_lines), "obs_re": obs_re, "obs_im": obs_im,
             "init_lines": tuple(init_lines), "uses_rho0_values": bool(uses_rho0_values),
+            "n_time_funcs": len(time_funcs), "time_lines_inline": tuple(time_inline),
+            "time_lines_exact": tuple(time_exact),
             "has_time": any(re.search(r"(?<![\w])t(?![\w])", ln) for ln in drive_lines)}
 
 
@@ -251,12 +281,20 @@ def model_source(frag, struct_name="Model"):
     static constexpr int NSTAT = {frag['n_static']};
     static constexpr int NDRV = {frag['n_drive']};
     static constexpr int NCONST = {frag['n_const']};
+    static constexpr int NTF = {frag.get('n_time_funcs', 0)};
     static constexpr bool kInitFromArray = {'true' if frag['uses_rho0_values'] else 'false'};
 
     __device__ __forceinline__ static void statics(double ParX, double ParY, double* __restrict__ Static_arr,
                                                    const double* __restrict__ Const_arr) {{
         (void)ParX; (void)ParY; (void)Static_arr; (void)Const_arr;
 {body(frag['static_lines'])}
+    }}
+
+    // the functions of time alone at time t, in FP64 (one evaluation serves every point)
+    __device__ __forceinline__ static void time_funcs(double t, const double* __restrict__ Const_d,
+                                                      double* __restrict__ Tf) {{
+        (void)t; (void)Const_d; (void)Tf;
+{body(frag.get('time_lines_exact', ()))}
     }}
 
     template <class F>
@@ -267,9 +305,25 @@ def model_source(frag, struct_name="Model"):
                                                   const typename F::real* __restrict__ Static_arr,
                                                   const double* __restrict__ Const_d,
                                                   const typename F::real* __restrict__ Const_arr) {{
+        double Tf[NTF > 0 ? NTF : 1];
+        (void)Tf;
+{body(frag.get('time_lines_inline', ()))}
+        drives_tf<F>(ParXd, ParYd, t, ParX, ParY, Drive_arr, Static_d, Static_arr, Const_d, Const_arr, Tf);
+    }}
+
+    // drives with the functions of time given (Tf, from time_funcs)
+    template <class F>
+    __device__ __forceinline__ static void drives_tf(double ParXd, double ParYd, double t,
+                                                     typename F::real ParX, typename F::real ParY,
+                                                     typename F::real* __restrict__ Drive_arr,
+                                                     const double* __restrict__ Static_d,
+                                                     const typename F::real* __restrict__ Static_arr,
+                                                     const double* __restrict__ Const_d,
+                                                     const typename F::real* __restrict__ Const_arr,
+                                                     const double* __restrict__ Tf) {{
         using R = typename F::real;
         (void)ParXd; (void)ParYd; (void)ParX; (void)ParY; (void)t; (void)Drive_arr;
-        (void)Static_d; (void)Static_arr; (void)Const_d; (void)Const_arr;
+        (void)Static_d; (void)Static_arr; (void)Const_d; (void)Const_arr; (void)Tf;
         double Dd[NDRV];
         (void)Dd;
 {body(frag['drive_lines'])}

@@ -276,3 +276,31 @@ def test_nonuniform_time_grid_is_rejected_before_gpu_launch():
         mesolve_2D(H, D, C, O, [0.0, 1.0], var_arrays=sweep, unroll="False")
     with pytest.raises(ValueError, match="precision must be"):
         mesolve_2D(H, D, C, O, [0.0, 1.0], var_arrays=sweep, precision="bf16")
+
+
+class TimeFunctionTests(unittest.TestCase):
+    """Functions of time alone in the drives become Tf[k] (evaluated once per warp by RK4), and the
+    runtime constants they read keep their values through the renumbering of used constants."""
+
+    def setUp(self):
+        cm = fake_device()
+        self.dev = cm.__enter__()
+        self.addCleanup(cm.__exit__, None, None, None)
+
+    def test_time_functions_and_constant_renumbering(self):
+        import re
+        eps, A, w, g, unused, t, Drive = sp.symbols("eps A w g unused t Drive", real=True)
+        sz, sx, sm = sp.Matrix([[1, 0], [0, -1]]), sp.Matrix([[0, 1], [1, 0]]), sp.Matrix([[0, 1], [0, 0]])
+        H = eps / 2 * sz + sp.Rational(1, 2) * sx + Drive * sz
+        mesolve_2D(H, A * sp.cos(w * t) + eps * sp.sin(2 * t), [sp.sqrt(g) * sm], sp.diag(0, 1),
+                   np.linspace(0, 1, 11), var_arrays={eps: np.array([-1., 1.]), A: np.array([0., 1.])},
+                   runtime_consts={w: 2.0, g: 0.01, unused: 5.0})
+        code, launch = self.dev.sources[-1], self.dev.launches[-1]
+        self.assertIn("static constexpr int NTF = 2;", code)
+        body = code[code.index("static void time_funcs"):code.index("template <class F>")]
+        k = int(re.search(r"cos\(t\*Const_d\[(\d+)\]\)", body).group(1))
+        self.assertEqual(launch.consts[k], 2.0)             # w, read only by a drive
+        self.assertIn("sin(2*t)", body)
+        refs = {int(m) for m in re.findall(r"Const_(?:arr|d)\[(\d+)\]", code)}
+        self.assertEqual(refs, set(range(len(launch.consts))))  # every index read has a value, none idle
+        self.assertNotIn(5.0, launch.consts)                 # the unused constant is dropped

@@ -39,9 +39,13 @@ def test_emitted_literals_use_ten_significant_digits():
                              A * sp.cos(sp.pi * t), [sp.sqrt(0.01) * sp.Matrix([[0, 1], [0, 0]])],
                              sp.diag(0, 1), [eps, A], RHSreuse=False)
     frag = emit.emit_model(c, False)
-    assert any("3.141592654e+00" in ln for ln in frag["drive_lines"])
-    assert any("F::cos(" in ln for ln in frag["drive_lines"])
-    assert all("M_PI" not in ln for ln in frag["drive_lines"] + frag["rhs_lines"])
+    # cos(pi t) depends on time alone: it is a time function Tf[0], printed for the per-point drives
+    # (phase-reduced, F::cos) and for the per-warp table (FP64)
+    assert frag["n_time_funcs"] == 1 and any("Tf[0]" in ln for ln in frag["drive_lines"])
+    assert any("3.141592654e+00" in ln and "F::cos(" in ln for ln in frag["time_lines_inline"])
+    assert any("3.141592654e+00" in ln and "gq::cos(" in ln for ln in frag["time_lines_exact"])
+    lines = frag["drive_lines"] + frag["rhs_lines"] + frag["time_lines_inline"] + frag["time_lines_exact"]
+    assert all("M_PI" not in ln for ln in lines)
     assert frag["state_size"] == 3
 
 
