@@ -23,13 +23,15 @@ def _calibrated(case, batch_levels, **extra):
 @pytest.mark.parametrize("name", ["c1_fp64_mean", "qubit_rk4_final"])
 def test_batched_calibration_matches_one_at_a_time(name):
     case = ref_cases.cases()[name]
-    tl = np.linspace(0.0, float(case["args"][4][-1]), 9)  # start from a coarse grid: several refinements
+    steps = len(case["args"][4]) - 1
+    tl = np.linspace(0.0, float(case["args"][4][-1]), steps // 8 + 1)  # coarse but stable: several refinements
     case = dict(case, args=tuple(case["args"][:4]) + (tl,))
     res1, info1 = _calibrated(case, 1)
     res3, info3 = _calibrated(case, 3)
     assert info1["steps"] == info3["steps"]
     d1, d3 = info1["details"], info3["details"]
-    assert d1["status"] == d3["status"]
+    assert d1["status"] == d3["status"] == "converged"
+    assert len(d1["tested"]) >= 2
     assert [t["steps"] for t in d1["tested"]] == [t["steps"] for t in d3["tested"]]
     assert [t["rms"] for t in d1["tested"]] == [t["rms"] for t in d3["tested"]]
     np.testing.assert_array_equal(res1, res3)
