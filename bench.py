@@ -116,12 +116,8 @@ def time_launches(torch, sweep, steps, warmup, flush):
 
 
 def _max_over_ranks(torch, value, ws):
-    if ws <= 1:
-        return value
-    import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from gqis.shard import max_over_ranks
+    return max_over_ranks(value) if ws > 1 else value
 
 
 def _barrier(ws):
@@ -206,9 +202,10 @@ def run_ours(args):
     from gqis import native, solver, workloads
 
     side, nsteps = args.side, args.nsteps
+    from gqis.shard import weak_axis
     w = workloads.four_level(side=None, steps=nsteps, duration=DURATION * nsteps / NSTEPS, full=side * ws)
     eps, A = w["symbols"]
-    eps_axis = w["var_arrays"][eps][rank * side:(rank + 1) * side]
+    eps_axis = weak_axis(w["var_arrays"][eps], ws, rank)  # this rank's 2048-row tile of the eps axis
     a_axis = np.linspace(0.0, 5.0, side)
     call = dict(var_arrays={eps: eps_axis, A: a_axis}, const_values={})
     model = (w["H"], w["Drive"], w["Col_Ops"], w["mean_operator"], w["tlist"])
@@ -470,7 +467,7 @@ def run_hilbert(args):
 
 
 def run_render(args):
-    """Phase-space rasteriser (SURVEY f-4): a 2048^2-point cloud resident on the device binned into a
+    """Phase-space rasteriser: a 2048^2-point cloud resident on the device binned into a
     512 x 512 mean-colour image each frame, then coloured into a 1920 x 1080 RGBA frame."""
     import numpy as np
     import torch
