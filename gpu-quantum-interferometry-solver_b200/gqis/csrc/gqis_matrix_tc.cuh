@@ -23,8 +23,9 @@
 // where the MMA is the longer part of a stage). Coefficients are evaluated once per point and
 // stage time by one thread and shared through shared memory. Jump terms come from per-thread
 // lists (the module's tcj_* tables) whose sources are populations rho_aa, shared through shared
-// memory when the stage input is written; element-wise terms off the diagonal (kWOffDiag) and
-// diagonal terms done in the epilogue read the stage input back from A (hi + lo).
+// memory when the stage input is written, or the thread's own element (element-wise terms on
+// coherences, kOwnTerms); those and the diagonal terms done in the epilogue read the stage input
+// back from A (hi + lo).
 // One thread polls the MMA's mbarrier (bounded); the CTA meets it at a barrier. On give-up the
 // CTA writes NaN outputs, waits (bounded) for the MMA in flight, frees its tensor memory and
 // returns.
@@ -281,7 +282,7 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
             }
         }
         float ur[E], ui[E];
-        if constexpr (MM::kWOffDiag || (T::NGM < MM::NG)) {  // terms that need the stage input itself
+        if constexpr (MM::kOwnTerms || (T::NGM < MM::NG)) {  // terms that need the stage input itself
             float a[8], b[8], c2[8], d2[8];
             gqtc::tmem_ld8(t_ahi + n0, a);
             gqtc::tmem_ld8(t_ahi + N + n0, b);
@@ -318,13 +319,6 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
             const Cx<float> kt = kbuf[(p * N + n) * LDK + j];  // K[j][n]
             kre[e] = Ki[e] + kt.im;                             // -i (K[n][j] - conj(K[j][n]))
             kim[e] = kt.re - Kr[e];
-            if constexpr (MM::kWOffDiag) {
-                if (n != j) {
-                    const Cx<float> w = ldc(MM::wjump(), n * N + j);
-                    kre[e] = fmaf(w.re, ur[e], fmaf(-w.im, ui[e], kre[e]));
-                    kim[e] = fmaf(w.re, ui[e], fmaf(w.im, ur[e], kim[e]));
-                }
-            }
         }
         // jump terms of this thread: population rho_aa of the stage input into row e
         float jre = 0.f, jim = 0.f;
@@ -337,17 +331,23 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
                 w.re *= cr;
                 w.im *= cr;
             }
-            const float x = rdiag[slot * P * N + p * N + __ldg(MM::tcj_a() + idx)];
-            if constexpr (MM::kJumpsOnDiagonal) {
+            const int a = __ldg(MM::tcj_a() + idx);
+            if constexpr (MM::kJumpsOnDiagonal && !MM::kOwnTerms) {
+                const float x = rdiag[slot * P * N + p * N + a];
                 jre = fmaf(w.re, x, jre);
                 jim = fmaf(w.im, x, jim);
             } else {
                 const int e = __ldg(MM::tcj_e() + idx);
+                const float x = (a >= 0) ? rdiag[slot * P * N + p * N + a] : 0.f;
 #pragma unroll
                 for (int ee = 0; ee < E; ++ee)
                     if (ee == e) {
-                        kre[ee] = fmaf(w.re, x, kre[ee]);
-                        kim[ee] = fmaf(w.im, x, kim[ee]);
+                        Cx<float> src = {x, 0.f};  // a population, or the element itself (a < 0)
+                        if constexpr (MM::kOwnTerms) {
+                            if (a < 0) src = {ur[ee], ui[ee]};
+                        }
+                        kre[ee] = fmaf(w.re, src.re, fmaf(-w.im, src.im, kre[ee]));
+                        kim[ee] = fmaf(w.re, src.im, fmaf(w.im, src.re, kim[ee]));
                     }
             }
         }

@@ -306,29 +306,36 @@ def _interleave(z):
 
 def tensor_core_jump_lists(mm: MatrixModel, rows_per_thread=8):
     """Jump terms of the tensor-core kernel grouped by thread: thread (column j, row block b)
-    owns rows b*8 .. b*8+7 of column j; each term is (row in block, source population a, coef,
-    rate index or -1). Element-wise terms on the diagonal become terms with a = own row.
-    Returns (lists[j][b], has_offdiagonal_elementwise)."""
+    owns rows b*8 .. b*8+7 of column j; each term is (row e in the block, source, coef, rate index
+    or -1). The source is a population index a >= 0 (rho_aa, shared between threads) or -1 for the
+    element (e, j) itself (element-wise terms on coherences, read back by the thread).
+    Returns (lists[j][b], has_own_element_terms)."""
     Np = mm.Np
     H = Np // rows_per_thread
     lists = [[[] for _ in range(H)] for _ in range(Np)]
+    own = False
+
+    def add(n, j, src_pop, coef, rate):
+        nonlocal own
+        if src_pop < 0:
+            own = True
+        lists[j][n // rows_per_thread].append((n % rows_per_thread, src_pop, complex(coef), rate))
+
     for dst, src, coef, rate in mm.jumps:
         n, j = divmod(dst, Np)
         a, b = divmod(src, Np)
-        if a != b:
-            raise ValueError("tensor-core jump lists need population sources")
-        lists[j][n // rows_per_thread].append((n % rows_per_thread, a, complex(coef), rate))
-    woff = False
+        if dst == src:
+            add(n, j, n if n == j else -1, coef, rate)
+        elif a == b:
+            add(n, j, a, coef, rate)
+        else:
+            raise ValueError("tensor-core jump lists need population or element-wise sources")
     for n in range(Np):
         for j in range(Np):
             w = complex(mm.wjump[n, j])
-            if w == 0:
-                continue
-            if n == j:
-                lists[j][n // rows_per_thread].append((n % rows_per_thread, n, w, -1))
-            else:
-                woff = True
-    return lists, woff
+            if w != 0:
+                add(n, j, n if n == j else -1, w, -1)
+    return lists, own
 
 
 def diag_in_mma(mm: MatrixModel):
@@ -339,7 +346,7 @@ def diag_in_mma(mm: MatrixModel):
 
 
 def _tensor_core_tables(mm: MatrixModel):
-    lists, woff = tensor_core_jump_lists(mm)
+    lists, own = tensor_core_jump_lists(mm)
     Np = mm.Np
     H = Np // 8
     jmax = max(1, max(len(lists[j][b]) for j in range(Np) for b in range(H)))
@@ -362,7 +369,7 @@ def _tensor_core_tables(mm: MatrixModel):
     ]
     on_diag = all(e + 8 * b == j for j in range(Np) for b in range(H) for (e, _, _, _) in lists[j][b])
     members = f"""    static constexpr int TCJ_MAX = {jmax};
-    static constexpr bool kWOffDiag = {'true' if woff else 'false'};
+    static constexpr bool kOwnTerms = {'true' if own else 'false'};
     static constexpr bool kJumpsOnDiagonal = {'true' if on_diag else 'false'};
     static constexpr bool kDiagInMma = {'true' if diag_in_mma(mm) else 'false'};
     __device__ __forceinline__ static const int* tcj_count() {{ return mm_tcj_count; }}
@@ -461,8 +468,8 @@ def tensor_core_blockers(mm: MatrixModel, form: str):
     elif 2 * mm.Np * (1 + mm.num_dense + (mm.num_diag if diag_in_mma(mm) else 0)) > 256:
         out.append(f"{mm.num_dense + mm.num_diag} coefficient operator terms exceed one MMA "
                    "(2 N (1 + terms) <= 256)")
-    if any(src // mm.Np != src % mm.Np for _, src, _, _ in mm.jumps):
-        out.append("a jump term reads an off-diagonal element (only populations may feed other elements)")
+    if any(src != dst and src // mm.Np != src % mm.Np for dst, src, _, _ in mm.jumps):
+        out.append("a jump term moves a coherence to another element (only populations may feed other elements)")
     elif mm.Np in TENSOR_DIMS:
         lists, _ = tensor_core_jump_lists(mm)
         if max(len(x) for col in lists for x in col) > 32:

@@ -108,3 +108,26 @@ def test_tensor_core_form_final_rho():
     ref = _oracle(w, kwargs, output_mode="final_rho")
     assert got.shape == ref.shape
     assert float(np.max(np.abs(got - ref))) <= 5e-6
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("form,tc", [("fp64", False), ("fp32", False), ("fp32", True)])
+def test_matrix_forms_with_runtime_rates_one_axis_and_rho0(form, tc):
+    """Runtime-constant collapse rates and Hamiltonian terms (the fit model), a one-axis sweep, a
+    numeric initial state and the `final` output, through the matrix kernels, against the reduced
+    form (FP64) of the same call."""
+    import sympy as sp
+    import gqis
+    from test_support_calls import qubit_fit_model
+    args, kwargs, (G1, Gp, D, A) = qubit_fit_model(side=(9, 5), steps=200, duration=10.0)
+    rho0 = sp.Matrix([[0.7, 0.2 - 0.1j], [0.2 + 0.1j, 0.3]])
+    eps = list(kwargs["var_arrays"])[0]
+    one_axis = dict(kwargs, var_arrays={eps: kwargs["var_arrays"][eps]}, rho0=rho0)
+    args1 = (args[0], args[1].subs(A, 0.8)) + args[2:]  # the drive amplitude fixed: one swept axis (eps)
+    for mode in ("mean", "final"):
+        ref = gqis.mesolve_2D(*args1, **one_axis, output_mode=mode, fp64=True, rhs_form="reduced")
+        got = gqis.mesolve_2D(*args1, **one_axis, output_mode=mode, precision=form,
+                              rhs_form="matrix_tc" if tc else "matrix")
+        assert got.shape == ref.shape == (9, 1)
+        tol = 1e-12 if form == "fp64" else 2e-6
+        assert float(np.max(np.abs(got - ref))) <= tol, (mode, float(np.max(np.abs(got - ref))))

@@ -109,3 +109,22 @@ def test_emitted_source_shape():
     assert "TR = 2, TC = 2, THREADS = 64;" in src
     with pytest.raises(ValueError):
         matrix_form.module_source(mm, "fp64", "mean_state", False)
+
+
+def test_tensor_core_jump_lists_of_a_dephased_qubit():
+    """sigma_z dephasing at a runtime rate acts element-wise on the coherences: those terms read the
+    thread's own element; relaxation feeds the ground population from the excited one."""
+    from gqis.rhs import runtime_const_values  # noqa: F401  (model preparation path)
+    eps, A, D, Drive, t, G1, Gp = sp.symbols("eps A Delta Drive t Gamma1 Gammaphi", real=True)
+    sz, sx, sm = sp.Matrix([[1, 0], [0, -1]]), sp.Matrix([[0, 1], [1, 0]]), sp.Matrix([[0, 1], [0, 0]])
+    mm, _ = matrix_form.compile_matrix_model(eps / 2 * sz + D / 2 * sx + Drive * sz, A * sp.cos(t),
+                                             [sp.sqrt(G1) * sm, sp.sqrt(Gp / 2) * sz], sp.diag(0, 1),
+                                             sweep_symbols=(eps, A), runtime_consts={G1: 0.01, Gp: 0.02, D: 1.0},
+                                             reuse=False)
+    lists, own = matrix_form.tensor_core_jump_lists(mm)
+    assert own
+    col1 = lists[1][0]  # column 1: rows 0 and 1
+    assert any(e == 0 and a == -1 and r >= 0 for e, a, c, r in col1)  # coherence (0, 1): own element, rate
+    assert any(e == 1 and a == 1 for e, a, c, r in col1)               # population (1, 1) from itself
+    assert any(e == 0 and a == 1 for e, a, c, r in lists[0][0])        # (0, 0) fed by rho_11 (relaxation)
+    assert matrix_form.tensor_core_blockers(mm, "fp32") == []

@@ -67,6 +67,23 @@ def matrix_calls():
     rho0 = np.zeros((4, 3, 16 * 16 - 1))
     out.append(("mesolve_2D", args, dict(kwargs, fp64=True, rhs_form="matrix", output_mode="final_rho",
                                          rho0_values=rho0)))
+    out += runtime_rate_calls()
+    return out
+
+
+def runtime_rate_calls():
+    """The fit model with one swept axis and a numeric rho0 through the matrix and reduced forms."""
+    import sympy as sp
+    args, kwargs, (G1, Gp, D, A) = qubit_fit_model(side=(9, 5), steps=200, duration=10.0)
+    rho0 = sp.Matrix([[0.7, 0.2 - 0.1j], [0.2 + 0.1j, 0.3]])
+    eps = list(kwargs["var_arrays"])[0]
+    one_axis = dict(kwargs, var_arrays={eps: kwargs["var_arrays"][eps]}, rho0=rho0)
+    args1 = (args[0], args[1].subs(A, 0.8)) + args[2:]
+    out = []
+    for mode in ("mean", "final"):
+        out.append(("mesolve_2D", args1, dict(one_axis, output_mode=mode, fp64=True, rhs_form="reduced")))
+        for form, rf in (("fp64", "matrix"), ("fp32", "matrix"), ("fp32", "matrix_tc")):
+            out.append(("mesolve_2D", args1, dict(one_axis, output_mode=mode, precision=form, rhs_form=rf)))
     return out
 
 
