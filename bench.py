@@ -545,6 +545,74 @@ def run_render(args):
     return 0
 
 
+def run_fit(args):
+    """Gradients of a time-averaged map (fit step): the checkpointed RK4 adjoint of a 256 x 256
+    two-level map, 4000 steps, d<O>avg / d(Gamma1, Gamma_phi, Delta), against the plain FP64 forward
+    sweep of the same map and central differences."""
+    import numpy as np
+    import torch
+    torch.cuda.set_device(0)
+    sys.path.insert(0, str(ROOT / "tests"))
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import gqis
+    from gqis import adjoint, solver
+    from test_support_calls import qubit_fit_model
+    fit_args, fit_kwargs, params = qubit_fit_model(side=(256, 256), steps=4000, duration=200.0)
+    params = list(params[:3])
+    prob = adjoint.Problem(*fit_args, **fit_kwargs, params=params)
+    fwd = solver.prepare_sweep("mesolve_2D", *fit_args, **fit_kwargs, fp64=True)
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, k):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        out = []
+        for _ in range(k):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            out.append(a.elapsed_time(b))
+        return float(np.mean(out))
+    sampler = ClockSampler(0).start()
+    ms_adj = timed(lambda: prob.run(), args.steps)
+    ms_fwd = timed(lambda: fwd.launch(stream), args.steps)
+    clocks = sampler.stop()
+    mean, grad = (x.cpu().numpy() for x in prob.run())
+    torch.cuda.synchronize()
+    plain = fwd.results[:, 0].double().cpu().numpy().reshape(256, 256)
+    sel = np.round(np.linspace(0, 255, 16)).astype(int)
+    es, As = list(fit_kwargs["var_arrays"])
+    sub = dict(fit_kwargs, var_arrays={es: fit_kwargs["var_arrays"][es][sel], As: fit_kwargs["var_arrays"][As][sel]})
+    errs = []
+    for m, prm in enumerate(params):
+        up, dn = dict(sub["runtime_consts"]), dict(sub["runtime_consts"])
+        up[prm] += 1e-6
+        dn[prm] -= 1e-6
+        fd = (gqis.mesolve_2D(*fit_args, **dict(sub, runtime_consts=up), fp64=True).real
+              - gqis.mesolve_2D(*fit_args, **dict(sub, runtime_consts=dn), fp64=True).real) / 2e-6
+        errs.append(float(np.max(np.abs(grad[np.ix_(sel, sel)][..., m] - fd)) / np.max(np.abs(fd))))
+    units = 256 * 256 * 4000
+    line = {
+        "metric": "gradient throughput: points*steps/s of the checkpointed RK4 adjoint (mean map + 3 parameter gradients)",
+        "value": units / (ms_adj / 1e3), "unit": "points*steps/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_adj, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "two-level driven qubit, 256x256 (eps, A) map, 4000 RK4 steps on [0, 200], "
+                               "params Gamma1, Gamma_phi, Delta (runtime constants), checkpoint every "
+                               f"{prob.checkpoint_every} steps", "l2": "not flushed (inputs are a few KB)"},
+        "forward_fp64_ms": ms_fwd, "adjoint_over_forward": ms_adj / ms_fwd,
+        "scratch_bytes": prob.scratch_bytes,
+        "mean_vs_plain_fp64_max_abs": float(np.max(np.abs(mean - plain))),
+        "grad_vs_central_fd_max_rel": dict(zip([str(p) for p in params], errs)),
+        "clocks": clocks, "gpu_launches": args.steps,
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def run_serving(args):
     """Config C5 (sweeps): Poisson stream of mixed-N, mixed-size sweep requests through the
     continuous-batching server (FP32 form), against the same requests one by one on plain FP64."""
@@ -668,7 +736,7 @@ def main():
     ap.add_argument("--forms", default="", help="hilbert: comma list of forms to run (e.g. matrix_tc_fp32); all if empty")
     ap.add_argument("--hsteps", type=int, default=2000, help="hilbert: RK4 steps (t spans 100 * hsteps / 2000)")
     ap.add_argument("--workload", default="four_level",
-                    choices=("four_level", "duffing", "serving", "hilbert", "render"),
+                    choices=("four_level", "duffing", "serving", "hilbert", "render", "fit"),
                     help="four_level: the headline RK4 interferogram; duffing: the adaptive ODE sweep")
     ap.add_argument("--solver", default="dop853a", help="adaptive solver of --workload duffing")
     args = ap.parse_args()
@@ -682,6 +750,8 @@ def main():
         return run_hilbert(args)
     if args.workload == "render":
         return run_render(args)
+    if args.workload == "fit":
+        return run_fit(args)
     return run_ours(args)
 
 
