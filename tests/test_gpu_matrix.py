@@ -7,7 +7,7 @@
 * the FP32 form against the same oracle: 2e-6 max-abs;
 * final_rho in the reduced layout, and rho0_values read back from it (a run split in two
   equals the run in one piece);
-* rhs_form="auto" picks the matrix form from N = 16 on (tensor cores for FP32);
+* rhs_form="auto" picks the matrix form from N = 8 on (tensor cores for FP32);
 * the tensor-core kernel (split-TF32 tcgen05 MMAs, FP32 accumulation and state) against the same
   oracle at N = 8, 16, 32: 5e-6 max-abs, and within 5e-6 of the CUDA-core FP32 form; final_rho
   through it as well. The grids leave the last tile of points partly empty.
@@ -77,9 +77,12 @@ def test_matrix_form_final_rho_and_rho0_values_continuation():
 
 
 @pytest.mark.gpu
-def test_auto_picks_matrix_form_from_n16():
+def test_auto_picks_reduced_below_n8_and_matrix_from_n8():
     import gqis
-    w, args, kwargs = hilbert_model(16)
+    args4, kwargs4 = serving_model(4, 8)
+    _, info = gqis.mesolve_2D(*args4, **kwargs4, precision="fp32", return_timing_info=True)
+    assert info["rhs_form"] == "reduced"
+    w, args, kwargs = hilbert_model(8)
     _, info = gqis.mesolve_2D(*args, **kwargs, precision="fp32", return_timing_info=True)
     assert info["rhs_form"] == "matrix_tc"
     _, info = gqis.mesolve_2D(*args, **kwargs, precision="fp64", return_timing_info=True)
