@@ -105,3 +105,17 @@ def test_solver_orders_rhs_counts_and_tableaus():
         get_solver_spec("tsit5", step_size=0.1, adaptive_options={"step_rtol": 1e-6})
     with pytest.raises(ValueError, match="Unknown adaptive_options"):
         get_solver_spec("tsit5a", adaptive_options={"rtol": 1e-6})
+
+
+@pytest.mark.parametrize("rhs_form,precision", [("matrix", "fp64"), ("matrix_tc", "fp32")])
+def test_density_matrix_modules_export_the_module_entry_points(rhs_form, precision):
+    """The density-matrix modules (CUDA-core and tcgen05) are model modules with the same C ABI."""
+    from gqis import workloads
+    w = workloads.n_level(16, side=2, steps=10, duration=1.0)
+    path = solver.prebuild("mesolve_2D", w["H"], w["Drive"], w["Col_Ops"], w["mean_operator"], w["tlist"],
+                           var_arrays=w["var_arrays"], precision=precision, rhs_form=rhs_form)
+    lib = ctypes.CDLL(str(path))
+    for name in ("gqis_model_info_get", "gqis_sweep_launch", "gqis_last_error", "gqis_sweep_launch_noalloc"):
+        assert hasattr(lib, name), name
+    src = Path(str(path).replace(".so", ".cu")).read_text()
+    assert ("#define GQ_MATRIX 2" in src) == (rhs_form == "matrix_tc")

@@ -37,10 +37,7 @@ def test_oracle_display_matches_reference_kernel():
 def test_render_library_exports_the_header_symbols():
     import re
     from gqis import native
-    path = native.lib_path("gqis_render")
-    if not path.exists():
-        pytest.skip("libgqis_render.so is built by __graft_entry__.build()")
-    lib = ctypes.CDLL(str(path))
+    lib = ctypes.CDLL(str(native.build("gqis_render")))  # nvcc builds it here; loading needs no GPU
     header = (ROOT / "include" / "gqis_render.h").read_text()
     names = re.findall(r"^(?:int|const char\*)\s+(gqis_\w+)\(", header, re.M)
     assert len(names) == 4
