@@ -54,8 +54,11 @@ struct RK4 {
         // Functions of time alone (M::NTF of them) are the same for every point: each warp evaluates
         // them for the stage times of kChunk steps at once into shared memory (lanes of the warp past
         // the end of the grid have exited, so the warp synchronises only its remaining lanes).
+        // Only for small models (S <= 35, N <= 6): there the drive's transcendental functions are a
+        // visible share of a step; larger reduced models spill, and the table-fill call inside the loop
+        // costs them more than it saves (measured at N = 8: 148 vs 110 ms in FP64).
         constexpr int kChunk = 16, kTimes = 2 * kChunk;
-        constexpr int NTF = M::NTF;
+        constexpr int NTF = (M::S <= 35) ? M::NTF : 0;
         __shared__ double tf_table[NTF > 0 ? GQ_BLOCK / 32 : 1][NTF > 0 ? kTimes * NTF : 1];
         double* const tab = tf_table[NTF > 0 ? (threadIdx.x >> 5) : 0];
         const int lane = threadIdx.x & 31;

@@ -26,9 +26,15 @@ struct Cx {
     R re, im;
 };
 
-template <class R>
-__device__ __forceinline__ Cx<R> ldc(const R* __restrict__ p, int i) {
-    return {__ldg(p + 2 * i), __ldg(p + 2 * i + 1)};
+// Complex entry i of an interleaved (re, im) array, one 8- or 16-byte load (the module's arrays
+// are 16-byte aligned).
+__device__ __forceinline__ Cx<float> ldc(const float* __restrict__ p, int i) {
+    const float2 v = __ldg(reinterpret_cast<const float2*>(p) + i);
+    return {v.x, v.y};
+}
+__device__ __forceinline__ Cx<double> ldc(const double* __restrict__ p, int i) {
+    const double2 v = __ldg(reinterpret_cast<const double2*>(p) + i);
+    return {v.x, v.y};
 }
 
 template <class R>

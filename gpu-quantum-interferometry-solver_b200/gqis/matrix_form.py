@@ -294,7 +294,7 @@ def _array(name, ctype, values, per_line=8):
     fmt = (lambda v: f"{float(v):.17e}") if ctype in ("double", "mreal") else (lambda v: str(int(v)))
     rows = [", ".join(fmt(v) for v in vals[i:i + per_line]) for i in range(0, len(vals), per_line)]
     body = ",\n    ".join(rows)
-    return f"__device__ const {ctype} {name}[{len(vals)}] = {{\n    {body}}};"
+    return f"__device__ __align__(16) const {ctype} {name}[{len(vals)}] = {{\n    {body}}};"
 
 
 def _interleave(z):
