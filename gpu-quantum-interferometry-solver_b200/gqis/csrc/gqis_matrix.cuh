@@ -49,7 +49,7 @@ constexpr size_t smem_bytes() {
     return (2 * (size_t)MM::N * MM::N + (size_t)MM::N * (MM::N + 1)) * sizeof(Cx<R>);
 }
 
-template <class MM, class F, int OUT>
+template <class MM, class F, int OUT, int TRACE>
 __global__ void __launch_bounds__(MM::THREADS) matrix_rk4_kernel(const gqis_sweep_desc d) {
     using R = typename F::real;
     constexpr int N = MM::N, NN = N * N, TR = MM::TR, TC = MM::TC, COLT = N / TC, LD = N + 1;
@@ -205,10 +205,34 @@ __global__ void __launch_bounds__(MM::THREADS) matrix_rk4_kernel(const gqis_swee
             }
     };
 
+    // Sum of (re, im) over the CTA, valid in thread 0 (the callers are uniform over the CTA; the
+    // buffer is reused only after further barriers).
+    __shared__ double red[2][MM::THREADS / 32];
+    auto cta_sum = [&](double& re, double& im) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            re += __shfl_xor_sync(0xffffffffu, re, off);
+            im += __shfl_xor_sync(0xffffffffu, im, off);
+        }
+        if ((tid & 31) == 0) {
+            red[0][tid >> 5] = re;
+            red[1][tid >> 5] = im;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            re = im = 0.0;
+            for (int w = 0; w < MM::THREADS / 32; ++w) {
+                re += red[0][w];
+                im += red[1][w];
+            }
+        }
+    };
+
     const double dt = d.dt, dt2d = dt * 0.5;
     const R h = (R)dt, h2 = (R)dt2d;
     const Coef<R> h6 = Coef<R>::make(dt / 6.0);
     double osum_re = 0.0, osum_im = 0.0;
+    int next_sample = d.trace_offset, sample = 0;  // observable trace, as the Recorder of gqfixed
 #pragma unroll
     for (int a = 0; a < TR; ++a)
 #pragma unroll
@@ -255,6 +279,20 @@ __global__ void __launch_bounds__(MM::THREADS) matrix_rk4_kernel(const gqis_swee
                 F::accumulate(y[a][b].im, cim[a][b], acc[a][b].im, h6);
             }
         if (OUT == GQIS_OUT_MEAN && step >= d.warmup_steps) observe(osum_re, osum_im);
+        if constexpr (TRACE == GQIS_TRACE_OBSERVABLE) {
+            if (step == next_sample) {
+                double tre = 0.0, tim = 0.0;
+                observe(tre, tim);
+                cta_sum(tre, tim);
+                if (tid == 0 && sample < d.num_trace) {
+                    R* tr = static_cast<R*>(d.trace) + ((size_t)local * d.num_trace + sample) * 2;
+                    tr[0] = (R)tre;
+                    tr[1] = (R)tim;
+                }
+                ++sample;
+                next_sample += d.trace_stride;
+            }
+        }
         if (step + 1 < d.num_steps) {  // k1 of the next step, at this step's end time
             write_stage(cur ^ 1, (R)0);
             cur ^= 1;
@@ -280,23 +318,9 @@ __global__ void __launch_bounds__(MM::THREADS) matrix_rk4_kernel(const gqis_swee
             }
     } else {
         if constexpr (OUT == GQIS_OUT_FINAL) observe(osum_re, osum_im);
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-            osum_re += __shfl_xor_sync(0xffffffffu, osum_re, off);
-            osum_im += __shfl_xor_sync(0xffffffffu, osum_im, off);
-        }
-        __shared__ double red[2][MM::THREADS / 32];
-        if ((tid & 31) == 0) {
-            red[0][tid >> 5] = osum_re;
-            red[1][tid >> 5] = osum_im;
-        }
-        __syncthreads();
+        cta_sum(osum_re, osum_im);
         if (tid == 0) {
-            double sr = 0.0, si = 0.0;
-            for (int w = 0; w < MM::THREADS / 32; ++w) {
-                sr += red[0][w];
-                si += red[1][w];
-            }
+            double sr = osum_re, si = osum_im;
             if constexpr (OUT == GQIS_OUT_MEAN) {
                 const double inv = 1.0 / (double)(d.num_steps - d.warmup_steps);
                 sr *= inv;

@@ -100,7 +100,7 @@ __device__ __forceinline__ float tf32_round(float x) {
     return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
 }
 
-template <class MM, int OUT>
+template <class MM, int OUT, int TRACE>
 __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) matrix_tc_kernel(const gqis_sweep_desc d) {
     using T = TcShape<MM>;
     using F = FormFP32;
@@ -366,6 +366,28 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
     const float h = (float)dt, h2 = (float)dt2d;
     const Coef<float> h6 = Coef<float>::make(dt / 6.0);
     double osum_re = 0.0, osum_im = 0.0;
+    // Sum of (re, im) over the threads of point p, valid in its lead thread: over the N columns (lanes
+    // p*N .. p*N+N-1 of a warp), then over the H row blocks through shared memory. Uniform over the CTA.
+    auto point_sum = [&](double& re, double& im) {
+#pragma unroll
+        for (int off = N / 2; off > 0; off >>= 1) {
+            re += __shfl_xor_sync(0xffffffffu, re, off);
+            im += __shfl_xor_sync(0xffffffffu, im, off);
+        }
+        if (j == 0) {
+            red[(0 * T::H + hh) * P + p] = re;
+            red[(1 * T::H + hh) * P + p] = im;
+        }
+        __syncthreads();
+        if (lead) {
+            re = im = 0.0;
+            for (int g = 0; g < T::H; ++g) {
+                re += red[(0 * T::H + g) * P + p];
+                im += red[(1 * T::H + g) * P + p];
+            }
+        }
+    };
+    int next_sample = d.trace_offset, sample = 0;  // observable trace, as the Recorder of gqfixed
     auto observe = [&]() {
 #pragma unroll
         for (int e = 0; e < E; ++e) {
@@ -404,6 +426,24 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
                     F::accumulate(yim[e], cim[e], aim[e], h6);
                 }
                 if (OUT == GQIS_OUT_MEAN && step >= d.warmup_steps) observe();
+                if constexpr (TRACE == GQIS_TRACE_OBSERVABLE) {
+                    if (step == next_sample) {
+                        double s_re = osum_re, s_im = osum_im;  // observe() adds into osum: keep it
+                        osum_re = osum_im = 0.0;
+                        observe();
+                        double tre = osum_re, tim = osum_im;
+                        osum_re = s_re;
+                        osum_im = s_im;
+                        point_sum(tre, tim);
+                        if (lead && active && sample < d.num_trace) {
+                            float* tr = static_cast<float*>(d.trace) + ((size_t)local * d.num_trace + sample) * 2;
+                            tr[0] = (float)tre;
+                            tr[1] = (float)tim;
+                        }
+                        ++sample;
+                        next_sample += d.trace_stride;
+                    }
+                }
                 if (step + 1 == d.num_steps) break;
 #pragma unroll
                 for (int e = 0; e < E; ++e) kre[e] = kim[e] = 0.f;
@@ -459,22 +499,9 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
         }
     } else {
         if constexpr (OUT == GQIS_OUT_FINAL) observe();
-#pragma unroll
-        for (int off = N / 2; off > 0; off >>= 1) {  // over the N columns of the point (lanes p*N ..)
-            osum_re += __shfl_xor_sync(0xffffffffu, osum_re, off);
-            osum_im += __shfl_xor_sync(0xffffffffu, osum_im, off);
-        }
-        if (j == 0) {
-            red[(0 * T::H + hh) * P + p] = osum_re;
-            red[(1 * T::H + hh) * P + p] = osum_im;
-        }
-        __syncthreads();
+        point_sum(osum_re, osum_im);
         if (lead && active) {
-            double sr = 0.0, si = 0.0;
-            for (int g = 0; g < T::H; ++g) {
-                sr += red[(0 * T::H + g) * P + p];
-                si += red[(1 * T::H + g) * P + p];
-            }
+            double sr = osum_re, si = osum_im;
             if constexpr (OUT == GQIS_OUT_MEAN) {
                 const double inv = 1.0 / (double)(d.num_steps - d.warmup_steps);
                 sr *= inv;

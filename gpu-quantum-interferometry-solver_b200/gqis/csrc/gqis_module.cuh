@@ -49,14 +49,14 @@ using Form = GQ_FORM;
 
 #if GQ_MATRIX == 2
 // Density-matrix form on the tensor cores (gqis_matrix_tc.cuh): one CTA per tile of 128 / N points.
-constexpr auto kKernel = gqmatrix_tc::matrix_tc_kernel<Model, GQ_OUT>;
+constexpr auto kKernel = gqmatrix_tc::matrix_tc_kernel<Model, GQ_OUT, GQ_TRACE>;
 constexpr int kBlock = gqmatrix_tc::TcShape<Model>::THREADS;
 constexpr size_t kSmem = gqmatrix_tc::TcShape<Model>::SMEM;
 constexpr int kPointsPerCta = gqmatrix_tc::TcShape<Model>::P;
 static_assert(Form::id == GQIS_FORM_FP32, "the tensor-core form is an FP32 form");
 #elif GQ_MATRIX
 // Density-matrix form (gqis_matrix.cuh, included by the generated source): one CTA per point.
-constexpr auto kKernel = gqmatrix::matrix_rk4_kernel<Model, Form, GQ_OUT>;
+constexpr auto kKernel = gqmatrix::matrix_rk4_kernel<Model, Form, GQ_OUT, GQ_TRACE>;
 constexpr int kBlock = Model::THREADS;
 constexpr size_t kSmem = gqmatrix::smem_bytes<Model, typename Form::real>();
 constexpr int kPointsPerCta = 1;

@@ -477,9 +477,11 @@ def tensor_core_blockers(mm: MatrixModel, form: str):
     return out
 
 
-def module_source(mm: MatrixModel, form: str, output_mode: str, uses_rho0_values: bool, tensor_cores=False):
+def module_source(mm: MatrixModel, form: str, output_mode: str, uses_rho0_values: bool, tensor_cores=False,
+                  trace=False):
     """Complete translation unit of one matrix-form module (C ABI of include/gqis_b200.h);
-    ``tensor_cores`` selects the tcgen05 kernel of csrc/gqis_matrix_tc.cuh."""
+    ``tensor_cores`` selects the tcgen05 kernel of csrc/gqis_matrix_tc.cuh, ``trace`` records the
+    observable every trace_stride steps."""
     if output_mode not in OUTPUT_IDS:
         raise ValueError(f"the matrix form supports the outputs {sorted(OUTPUT_IDS)}, not '{output_mode}'")
     if tensor_cores:
@@ -502,7 +504,7 @@ def module_source(mm: MatrixModel, form: str, output_mode: str, uses_rho0_values
         "#define GQ_SOLVER_ID 0",
         "#define GQ_ADAPTIVE 0",
         f"#define GQ_OUT {OUTPUT_IDS[output_mode]}",
-        "#define GQ_TRACE 0",
+        f"#define GQ_TRACE {1 if trace else 0}",
         f"#define GQ_MODEL_HASH 0x{model_hash:016x}ULL",
         '#include "gqis_module.cuh"',
         "",

@@ -451,7 +451,7 @@ def _solve_symbolic_system(H, Drive, Col_Ops, mean_operator, tlist,
     include directory (or a file in it) searched before the packaged CUDA templates, and
     ``rhs_form``: ``"reduced"`` (the reference's N*N-1 real equations), ``"matrix"`` (the
     density-matrix kernel of ``matrix_form`` on the CUDA cores; fixed-step RK4, outputs
-    ``mean``/``final``/``final_rho``, no time trace), ``"matrix_tc"`` (the same on the tensor
+    ``mean``/``final``/``final_rho`` and the observable time trace), ``"matrix_tc"`` (the same on the tensor
     cores, split-TF32 operands with FP32 accumulation; FP32 form, padded N of 8, 16 or 32) or
     ``"auto"`` (matrix from N = 8 on where it applies, on the tensor cores for FP32 sweeps the
     tensor-core kernel can run).
@@ -565,11 +565,11 @@ def _solve_symbolic_system(H, Drive, Col_Ops, mean_operator, tlist,
 
     if rhs_form not in ("auto", "reduced", "matrix", "matrix_tc"):
         raise ValueError("rhs_form must be 'auto', 'reduced', 'matrix' or 'matrix_tc'.")
-    matrix_ok = (compiled_rhs is None and _ode_size is None and spec.name == "rk4" and not return_time_trace
+    matrix_ok = (compiled_rhs is None and _ode_size is None and spec.name == "rk4" and not _state_trace
                  and mode in ("mean", "final", "final_rho"))
     if rhs_form in ("matrix", "matrix_tc") and not matrix_ok:
-        raise ValueError(f"rhs_form='{rhs_form}' needs a Lindblad model given symbolically, solver='rk4', "
-                         "output_mode 'mean', 'final' or 'final_rho' and no time trace.")
+        raise ValueError(f"rhs_form='{rhs_form}' needs a Lindblad model given symbolically, solver='rk4' "
+                         "and output_mode 'mean', 'final' or 'final_rho'.")
     use_matrix = rhs_form in ("matrix", "matrix_tc") or (rhs_form == "auto" and matrix_ok and H is not None
                                                          and H.shape[0] >= MATRIX_FORM_FROM)
     tensor_cores = rhs_form == "matrix_tc"
@@ -634,7 +634,8 @@ def _solve_symbolic_system(H, Drive, Col_Ops, mean_operator, tlist,
     entry = _KERNEL_CACHE.get(kkey) if RHSreuse else None
     if entry is None:
         from . import engine
-        source = (matrix_form.module_source(compiled, form, mode, bool(uses_rho0_values), tensor_cores)
+        source = (matrix_form.module_source(compiled, form, mode, bool(uses_rho0_values), tensor_cores,
+                                            trace=trace_mode == "observable")
                   if use_matrix
                   else engine.module_source(frag, spec, form, mode, trace_mode, unroll))
         entry = {"source": source,

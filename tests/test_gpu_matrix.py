@@ -134,3 +134,22 @@ def test_matrix_forms_with_runtime_rates_one_axis_and_rho0(form, tc):
         assert got.shape == ref.shape == (9, 1)
         tol = 1e-12 if form == "fp64" else 2e-6
         assert float(np.max(np.abs(got - ref))) <= tol, (mode, float(np.max(np.abs(got - ref))))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("form,rhs_form,tol", [("fp64", "matrix", 1e-12), ("fp32", "matrix", 2e-6),
+                                               ("fp32", "matrix_tc", 2e-6)])
+def test_matrix_forms_record_the_observable_trace(form, rhs_form, tol):
+    """return_time_trace through the density-matrix kernels: the same samples (every k-th step) as the
+    reduced form's trace (FP64), and the same final map."""
+    import gqis
+    args, kwargs = serving_model(8, 6)
+    args = args[:4] + (np.linspace(0.0, 5.0, 101),)
+    ref_map, ref_tr, ref_t = gqis.mesolve_2D(*args, **kwargs, fp64=True, rhs_form="reduced",
+                                             return_time_trace=True, time_trace_every=7)
+    got_map, got_tr, got_t = gqis.mesolve_2D(*args, **kwargs, precision=form, rhs_form=rhs_form,
+                                             return_time_trace=True, time_trace_every=7)
+    assert got_tr.shape == ref_tr.shape == (6, 6, 15)
+    np.testing.assert_allclose(got_t, ref_t, rtol=1e-6)
+    assert float(np.max(np.abs(got_tr - ref_tr))) <= tol
+    assert float(np.max(np.abs(got_map - ref_map))) <= tol

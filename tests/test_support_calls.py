@@ -68,6 +68,12 @@ def matrix_calls():
     out.append(("mesolve_2D", args, dict(kwargs, fp64=True, rhs_form="matrix", output_mode="final_rho",
                                          rho0_values=rho0)))
     out += runtime_rate_calls()
+    args, kwargs = serving_model(8, 6)  # observable traces through the matrix kernels
+    args = args[:4] + (np.linspace(0.0, 5.0, 101),)
+    trace = dict(kwargs, return_time_trace=True, time_trace_every=7)
+    out.append(("mesolve_2D", args, dict(trace, fp64=True, rhs_form="reduced")))
+    for form, rf in (("fp64", "matrix"), ("fp32", "matrix"), ("fp32", "matrix_tc")):
+        out.append(("mesolve_2D", args, dict(trace, precision=form, rhs_form=rf)))
     return out
 
 
