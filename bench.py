@@ -401,7 +401,7 @@ def run_hilbert(args):
         w = workloads.n_level(N, side=64, steps=steps, duration=100.0 * steps / 2000)
         model = (w["H"], w["Drive"], w["Col_Ops"], w["mean_operator"], w["tlist"])
         points = 64 * 64
-        forms = [("matrix", "fp64"), ("matrix", "fp32")] + ([("matrix_tc", "fp32")] if N <= 32 else []) + \
+        forms = [("matrix", "fp64"), ("matrix", "fp32")] + [("matrix_tc", "fp32")] + \
                 ([("reduced", "fp64"), ("reduced", "fp32")] if N <= 8 else [])
         if args.forms:
             forms = [f for f in forms if f"{f[0]}_{f[1]}" in args.forms.split(",")]

@@ -1,15 +1,22 @@
 // gqis_matrix_tc.cuh - density-matrix Lindblad sweep on the sm_100a tensor cores (tcgen05).
 //
 // Same master equation, RK4 stage structure and outputs as gqis_matrix.cuh (the CUDA-core
-// form), with the operator products on the tensor cores. One CTA integrates a tile of
-// P = 128 / N points (N = padded dimension 8, 16 or 32); the tile is one M = 128 MMA:
+// form), with the operator products on the tensor cores. A tile of P = 128 / N points
+// (N = padded dimension 8, 16, 32 or 64) is one M = 128 MMA:
 //
 //   row r = p*N + j  (point p of the tile, column j of its rho)  = tensor-memory lane r
 //   A[r][k]   = Re rho_p[k][j] (k < N),  Im rho_p[k-N][j] (k >= N)        (tensor memory)
 //   B[k][col] = real embedding of T_q^T for the operator terms           (shared memory)
 //               T_0 = Heff0, T_q = M_q (dense, q = 1..ND), T_{ND+g} = diag(v_g) (g = 1..NG)
-//               col = (2q + c) N + n, c = 0 (Re) / 1 (Im)
+//               col = (2q + c) NH + n - nb, c = 0 (Re) / 1 (Im)
 //   D[r][col] = Re/Im (T_q rho_p)[n][j]                                    (tensor memory)
+//
+// Up to N = 32 one CTA holds the tile (NH = N rows n of every column, nb = 0). At N = 64 the
+// tile's state does not fit one SM's registers, so a cluster of CL = 2 CTAs shares it: CTA c owns
+// rows n in [nb, nb + NH), nb = c NH, NH = N / 2, of every column, multiplies with the B columns of
+// its rows only, and both CTAs keep the whole stage input in A. Each stage the CTAs swap their
+// halves of the stage input and the parts of K the other one reads transposed through distributed
+// shared memory (plain remote stores, then the cluster barrier).
 //
 // One MMA chain gives every point's T_q rho at once; the epilogue forms K = sum_q c_q(t) T_q rho
 // with the point's FP64-evaluated coefficients (c_0 = 1), -i (K - K^dag) through a transposed
@@ -18,17 +25,18 @@
 // (hi*hi + hi*lo + lo*hi) with FP32 accumulation; the state is FP32 with the FP32 form's
 // compensated update, time and coefficients FP64, the mean of <O> FP64.
 //
-// Thread t: lane r = t % 128 (warp quadrant r / 32), rows n0 = 8 (t / 128) .. n0 + 7 of column j.
+// Thread t: lane r = t % 128 (warp quadrant r / 32), rows n0 = nb + 8 (t / 128) .. n0 + 7 of column j.
 // Diagonal operator terms go through the MMA (kDiagInMma, small N) or the epilogue (larger N,
-// where the MMA is the longer part of a stage). Coefficients are evaluated once per point and
-// stage time by one thread and shared through shared memory. Jump terms come from per-thread
+// where the MMA is the longer part of a stage). Coefficients are evaluated in FP64 for every point
+// and stage time of KB steps at once, spread over all threads while an MMA runs, into a
+// double-buffered table in shared memory. Jump terms come from per-thread
 // lists (the module's tcj_* tables) whose sources are populations rho_aa, shared through shared
 // memory when the stage input is written, or the thread's own element (element-wise terms on
 // coherences, kOwnTerms); those and the diagonal terms done in the epilogue read the stage input
 // back from A (hi + lo).
 // One thread polls the MMA's mbarrier (bounded); the CTA meets it at a barrier. On give-up the
-// CTA writes NaN outputs, waits (bounded) for the MMA in flight, frees its tensor memory and
-// returns.
+// CTA (both CTAs of a cluster, which learn of it at their next cluster barrier) writes NaN outputs,
+// waits (bounded) for the MMA in flight, frees its tensor memory and returns.
 #pragma once
 
 #include <type_traits>
@@ -46,17 +54,22 @@ constexpr uint32_t kMaxPolls = 1u << 20;  // mbarrier polls before a wait gives 
 template <class MM>
 struct TcShape {
     static constexpr int N = MM::N;
+    static constexpr int CL = N == 64 ? 2 : 1;  // CTAs per tile (cluster size)
+    static constexpr int NH = N / CL;         // rows n of every column held by one CTA
     static constexpr int P = 128 / N;         // points per tile
     static constexpr int E = 8;               // rows of a column per thread
-    static constexpr int H = N / E;           // threads per column
+    static constexpr int H = NH / E;          // threads per column in one CTA
     static constexpr int THREADS = 128 * H;
     static constexpr int MIN_CTAS = 65536 / (THREADS * 128);  // keeps <= 128 registers per thread
     static constexpr int NGM = MM::kDiagInMma ? MM::NG : 0;  // diagonal terms done by the MMA
     static constexpr int NT = 1 + MM::ND + NGM;      // operator terms in B
-    static constexpr int NMMA = 2 * N * NT;   // B / D columns
+    static constexpr int NMMA = 2 * NH * NT;  // B / D columns
     static constexpr int KDIM = 2 * N;        // real-embedded inner dimension
     static constexpr int KCH = KDIM / 8;      // MMA K steps of 8 TF32
     static constexpr int NC = MM::NCOEF > 0 ? MM::NCOEF : 1;
+    static constexpr int CG = N > 32 ? N / 32 : 1;  // warps spanned by one column set (point sums)
+    static constexpr int KB = 8;              // steps per block of the coefficient table
+    static constexpr int TS = 3 * KB;         // table slots per block: start, midpoint and end of each step
     static constexpr int COL_D = 0, COL_AHI = NMMA, COL_ALO = NMMA + KDIM;
     static constexpr int COLS_USED = NMMA + 2 * KDIM;
     static constexpr int TMEM_COLS = COLS_USED <= 32 ? 32 : COLS_USED <= 64 ? 64 : COLS_USED <= 128 ? 128
@@ -66,21 +79,24 @@ struct TcShape {
     static constexpr size_t B_BYTES = (size_t)NMMA * KDIM * 4;
     static constexpr size_t OFF_BHI = 0, OFF_BLO = B_BYTES;
     static constexpr size_t OFF_K = 2 * B_BYTES;
-    static constexpr size_t K_BYTES = (size_t)P * N * LDK * 8;
-    static constexpr size_t OFF_RD = OFF_K + K_BYTES;           // [2][P*N] populations of the stage input
+    static constexpr size_t K_BYTES = (size_t)P * NH * LDK * 8;  // K[j][n] for the CTA's rows n, every j
+    static constexpr size_t OFF_X = OFF_K + K_BYTES;            // [P][H][E][N] the partner's stage input
+    static constexpr size_t X_BYTES = CL > 1 ? (size_t)P * H * E * N * 8 : 0;
+    static constexpr size_t OFF_RD = OFF_X + X_BYTES;           // [2][P*N] populations of the stage input
     static constexpr size_t RD_BYTES = 2 * (size_t)P * N * 4;
-    static constexpr size_t OFF_CS = OFF_RD + RD_BYTES;         // [2][P][NC] coefficients
-    static constexpr size_t CS_BYTES = 2 * (size_t)P * NC * 4;
+    static constexpr size_t OFF_CS = OFF_RD + RD_BYTES;         // [2][TS][P][NC] coefficient table
+    static constexpr size_t CS_BYTES = 2 * (size_t)TS * P * NC * 4;
     static constexpr size_t OFF_RED = (OFF_CS + CS_BYTES + 7) / 8 * 8;
-    static constexpr size_t RED_BYTES = 2 * (size_t)H * P * 8;
-    static constexpr size_t OFF_MISC = OFF_RED + RED_BYTES;
+    static constexpr size_t RED_BYTES = 2 * (size_t)H * CG * P * 8 + 2 * (size_t)P * 8;  // + the partner's sums
+    static constexpr size_t OFF_MISC = OFF_RED + RED_BYTES;     // mbarrier, tensor-memory slot, failure flag
     static constexpr size_t NEEDED = OFF_MISC + 64;
     // At most 512 / TMEM_COLS CTAs can hold tensor memory on one SM: pad the shared memory so that
     // no more CTAs fit (228 KB per SM, 1 KB reserved per CTA) and no allocation ever waits.
     static constexpr int MAX_CTAS = 512 / TMEM_COLS;
     static constexpr size_t FLOOR = 233472 / (MAX_CTAS + 1) + 1;
     static constexpr size_t SMEM = ((NEEDED > FLOOR ? NEEDED : FLOOR) + 1023) / 1024 * 1024;
-    static_assert(N == 8 || N == 16 || N == 32, "tensor-core form: padded dimension 8, 16 or 32");
+    static_assert(N == 8 || N == 16 || N == 32 || N == 64, "tensor-core form: padded dimension 8, 16, 32 or 64");
+    static_assert(H >= 1 && NH % E == 0, "rows per thread");
     static_assert(NMMA % 16 == 0 && NMMA <= 256, "MMA N dimension");
     static_assert(COLS_USED <= 512, "tensor memory columns");
     static_assert(SMEM <= 232448, "shared memory per CTA");
@@ -104,39 +120,40 @@ template <class MM, int OUT, int TRACE>
 __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) matrix_tc_kernel(const gqis_sweep_desc d) {
     using T = TcShape<MM>;
     using F = FormFP32;
-    constexpr int N = T::N, P = T::P, E = T::E, LDK = T::LDK, NO = MM::NO, NC = T::NC;
+    constexpr int N = T::N, P = T::P, E = T::E, LDK = T::LDK, NO = MM::NO, NC = T::NC, NH = T::NH, H = T::H;
     static_assert(std::is_same<typename MM::real, float>::value, "tensor-core form uses FP32 model data");
     extern __shared__ __align__(1024) unsigned char gq_smem[];
     float* const bhi = reinterpret_cast<float*>(gq_smem + T::OFF_BHI);
     float* const blo = reinterpret_cast<float*>(gq_smem + T::OFF_BLO);
     Cx<float>* const kbuf = reinterpret_cast<Cx<float>*>(gq_smem + T::OFF_K);
+    float2* const xbuf = reinterpret_cast<float2*>(gq_smem + T::OFF_X);
     float* const rdiag = reinterpret_cast<float*>(gq_smem + T::OFF_RD);
     float* const cs = reinterpret_cast<float*>(gq_smem + T::OFF_CS);
     double* const red = reinterpret_cast<double*>(gq_smem + T::OFF_RED);
     uint64_t* const bar = reinterpret_cast<uint64_t*>(gq_smem + T::OFF_MISC);
     uint32_t* const tslot = reinterpret_cast<uint32_t*>(gq_smem + T::OFF_MISC + 8);
+    uint32_t* const fail_flag = reinterpret_cast<uint32_t*>(gq_smem + T::OFF_MISC + 12);  // set by the partner
 
     const int tid = threadIdx.x;
     const int r = tid & 127;
     const int hh = tid >> 7;
     const int p = r / N, j = r % N;
-    const int n0 = hh * E;
+    const int crank = T::CL > 1 ? (int)gqtc::cluster_ctarank() : 0;
+    const int nb = crank * NH;   // first row of this CTA
+    const int n0 = nb + hh * E;  // first row of this thread
     const int warp = tid >> 5;
     const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
-    const bool lead = (j == 0) && (hh == 0);  // evaluates the point's coefficients
+    const bool lead = (j == 0) && (hh == 0);  // holds the point's sums (in each CTA)
 
-    const int64_t local = (int64_t)blockIdx.x * P + p;
+    const int64_t tile = (int64_t)(blockIdx.x / T::CL);
+    const int64_t local = tile * P + p;
     const bool active = local < d.point_count;
     const int64_t lp = active ? local : d.point_count - 1;  // idle rows integrate a copy of the last point
-    const int64_t gp = d.point_begin + lp;
-    const int ix = (int)(gp / d.num_y);
-    const int iy = (int)(gp - (int64_t)ix * d.num_y);
-    const double Xd = d.par_x[ix], Yd = d.par_y[iy];
 
     // ---- B = split-TF32 real embedding of the operator terms; mbarrier; tensor memory
     for (int e = tid; e < T::NMMA * T::KDIM; e += T::THREADS) {
         const int col = e / T::KDIM, k = e % T::KDIM;
-        const int q = col / (2 * N), c = (col / N) & 1, n = col % N;
+        const int q = col / (2 * NH), c = (col / NH) & 1, n = nb + col % NH;
         const int m = k % N;
         const bool imag_in = k >= N;
         float tr, ti;
@@ -157,7 +174,10 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
         blo[off] = lo;
     }
     gqtc::fence_proxy_async_smem();
-    if (tid == 0) gqtc::mbar_init(bar, 1);
+    if (tid == 0) {
+        gqtc::mbar_init(bar, 1);
+        *fail_flag = 0u;
+    }
     if (warp == 0) {
         gqtc::tmem_alloc(tslot, T::TMEM_COLS);
         gqtc::tmem_relinquish();
@@ -165,6 +185,18 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
     gqtc::fence_before_sync();
     __syncthreads();
     gqtc::fence_after_sync();
+    // the partner CTA's buffers (distributed shared memory); both CTAs run before either writes there
+    Cx<float>* kbuf_peer = kbuf;
+    float2* xbuf_peer = xbuf;
+    double* red_peer = red;
+    uint32_t* flag_peer = fail_flag;
+    if constexpr (T::CL > 1) {
+        kbuf_peer = gqtc::cluster_peer(kbuf, (uint32_t)(crank ^ 1));
+        xbuf_peer = gqtc::cluster_peer(xbuf, (uint32_t)(crank ^ 1));
+        red_peer = gqtc::cluster_peer(red, (uint32_t)(crank ^ 1));
+        flag_peer = gqtc::cluster_peer(fail_flag, (uint32_t)(crank ^ 1));
+        gqtc::cluster_sync();
+    }
     const uint32_t tbase = *tslot;
     const uint32_t t_d = tbase + T::COL_D + lane_base;
     const uint32_t t_ahi = tbase + T::COL_AHI + lane_base;
@@ -207,22 +239,41 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
             are[e] = aim[e] = 0.f;
         }
     }
-    const int jl = j * T::H + hh;  // this thread's jump list
+    const int jl = j * (N / E) + n0 / E;  // this thread's jump list (column j, row block n0 / 8)
     const int jcount = __ldg(MM::tcj_count() + jl);
 
-    // coefficients of the point at time t into slot `v` (lead thread only)
-    auto coef = [&](double t, int v) {
-        if (lead) {
+    const double dt = d.dt, dt2d = dt * 0.5;
+    // Coefficient table of block b (steps b KB .. b KB + KB - 1) into buffer b & 1: for every point of
+    // the tile and step n the coefficients at the stage times of gqfixed::RK4 - slot 3 i: the step's
+    // start (t_in + 0 for n = 0, else the previous step's end), 3 i + 1: t_mid = (n + 1/2) dt,
+    // 3 i + 2: t_mid + dt/2. All threads share the work; a thread evaluates at most a few entries.
+    auto fill_table = [&](int b) {
+        for (int idx = tid; idx < T::TS * P; idx += T::THREADS) {
+            const int slot = idx / P, pp = idx - slot * P;
+            const int n = b * T::KB + slot / 3, kind = slot % 3;
+            double t;
+            if (kind == 0)
+                t = (n == 0) ? d.t_in + 0.0 : d.t_in + ((((double)(n - 1) + 0.5) * dt) + dt2d);
+            else if (kind == 1)
+                t = d.t_in + ((double)n + 0.5) * dt;
+            else
+                t = d.t_in + ((((double)n + 0.5) * dt) + dt2d);
+            int64_t lq = tile * P + pp;
+            if (lq >= d.point_count) lq = d.point_count - 1;
+            const int64_t gq = d.point_begin + lq;
+            const int qx = (int)(gq / d.num_y);
+            const int qy = (int)(gq - (int64_t)qx * d.num_y);
             double Cd[MM::NCONST], c[NC];
 #pragma unroll
             for (int i = 0; i < MM::NCONST; ++i) Cd[i] = d.consts ? __ldg(d.consts + i) : 0.0;
-            MM::coef(t, Xd, Yd, Cd, c);
+            MM::coef(t, __ldg(d.par_x + qx), __ldg(d.par_y + qy), Cd, c);
 #pragma unroll
-            for (int q = 0; q < MM::NCOEF; ++q) cs[(v * P + p) * NC + q] = (float)c[q];
+            for (int q = 0; q < MM::NCOEF; ++q) cs[(((b & 1) * T::TS + slot) * P + pp) * NC + q] = (float)c[q];
         }
     };
 
-    // stage input u = y + s k -> A (hi / lo TF32 parts); populations -> rdiag[slot]
+    // stage input u = y + s k -> A (hi / lo TF32 parts); populations -> rdiag[slot]; in a cluster
+    // also into the partner's exchange buffer (its rows of A are this CTA's rows)
     auto write_stage = [&](float s, const float (&kre)[E], const float (&kim)[E], int slot) {
         float hr[E], hi_[E], lr[E], li[E];
 #pragma unroll
@@ -233,6 +284,7 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
             lr[e] = ur - hr[e];  // |lo| <= 2^-11 |u|; its TF32 read loses at most 2^-21 |u|
             li[e] = ui - hi_[e];
             if (n0 + e == j) rdiag[slot * P * N + p * N + j] = ur;
+            if constexpr (T::CL > 1) xbuf_peer[((p * H + hh) * E + e) * N + j] = make_float2(ur, ui);
         }
         gqtc::tmem_st8(t_ahi + n0, hr);
         gqtc::tmem_st8(t_ahi + N + n0, hi_);
@@ -241,8 +293,28 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
     };
 
     uint32_t phase = 0;
-    // k = f(u) for the stage input in A; false when the MMA wait gave up (uniform over the CTA).
-    auto eval = [&](float (&kre)[E], float (&kim)[E], int slot, int v) -> bool {
+    // k = f(u) for the stage input in A with the coefficients of table entry v; false when the MMA wait
+    // gave up (uniform over the CTA and the cluster). While the MMA runs, the threads fill the
+    // coefficient table of block `fill` (if >= 0).
+    auto eval = [&](float (&kre)[E], float (&kim)[E], int slot, int v, int fill) -> bool {
+        if constexpr (T::CL > 1) {
+            gqtc::cluster_sync();  // the partner's half of the stage input is in xbuf
+            const int mb = (crank ^ 1) * NH + hh * E;
+            float hr[E], hi_[E], lr[E], li[E];
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const float2 u = xbuf[((p * H + hh) * E + e) * N + j];
+                hr[e] = tf32_round(u.x);
+                hi_[e] = tf32_round(u.y);
+                lr[e] = u.x - hr[e];
+                li[e] = u.y - hi_[e];
+                if (mb + e == j) rdiag[slot * P * N + p * N + j] = u.x;
+            }
+            gqtc::tmem_st8(t_ahi + mb, hr);
+            gqtc::tmem_st8(t_ahi + N + mb, hi_);
+            gqtc::tmem_st8(t_alo + mb, lr);
+            gqtc::tmem_st8(t_alo + N + mb, li);
+        }
         gqtc::tmem_wait_st();
         gqtc::fence_before_sync();
         __syncthreads();  // stage input complete in A; coefficients and populations written
@@ -259,64 +331,77 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
             }
             gqtc::mma_commit(bar);
         }
+        if (fill >= 0) fill_table(fill);  // the other buffer was last read a block ago
         float cq[T::NT];  // the point's coefficients of the operator terms (c_0 = 1)
         cq[0] = 1.f;
 #pragma unroll
         for (int q = 1; q < T::NT; ++q) cq[q] = cs[(v * P + p) * NC + (q - 1)];
         // one thread polls the mbarrier; the others wait at the barrier instead of spinning
         const bool ok = (tid != 0) || gqtc::mbar_wait_bounded(bar, phase, kMaxPolls);
-        if (__syncthreads_or(!ok)) return false;  // MMA complete (or given up, uniformly)
-        phase ^= 1u;
-        gqtc::fence_after_sync();
-        float Kr[E], Ki[E];
-#pragma unroll
-        for (int q = 0; q < T::NT; ++q) {
-            float a[8], b[8];
-            gqtc::tmem_ld8(t_d + (2 * q) * N + n0, a);
-            gqtc::tmem_ld8(t_d + (2 * q + 1) * N + n0, b);
-            gqtc::tmem_wait_ld();
-#pragma unroll
-            for (int e = 0; e < E; ++e) {
-                Kr[e] = (q == 0) ? a[e] : fmaf(cq[q], a[e], Kr[e]);
-                Ki[e] = (q == 0) ? b[e] : fmaf(cq[q], b[e], Ki[e]);
-            }
+        const bool bad = __syncthreads_or(!ok);  // MMA complete (or given up, uniformly over the CTA)
+        if constexpr (T::CL == 1) {
+            if (bad) return false;
         }
-        float ur[E], ui[E];
-        if constexpr (MM::kOwnTerms || (T::NGM < MM::NG)) {  // terms that need the stage input itself
-            float a[8], b[8], c2[8], d2[8];
-            gqtc::tmem_ld8(t_ahi + n0, a);
-            gqtc::tmem_ld8(t_ahi + N + n0, b);
-            gqtc::tmem_ld8(t_alo + n0, c2);
-            gqtc::tmem_ld8(t_alo + N + n0, d2);
-            gqtc::tmem_wait_ld();
+        float Kr[E], Ki[E], ur[E], ui[E];
+        if (!bad) {  // (a cluster CTA whose wait gave up skips to the barrier that tells the partner)
+            phase ^= 1u;
+            gqtc::fence_after_sync();
 #pragma unroll
-            for (int e = 0; e < E; ++e) {
-                ur[e] = a[e] + c2[e];
-                ui[e] = b[e] + d2[e];
-            }
-        }
-        if constexpr (T::NGM < MM::NG) {  // diagonal terms in the epilogue: K += (sum_g c_g v_g[n]) u[n][j]
+            for (int q = 0; q < T::NT; ++q) {
+                float a[8], b[8];
+                gqtc::tmem_ld8(t_d + (2 * q) * NH + (n0 - nb), a);
+                gqtc::tmem_ld8(t_d + (2 * q + 1) * NH + (n0 - nb), b);
+                gqtc::tmem_wait_ld();
 #pragma unroll
-            for (int e = 0; e < E; ++e) {
-                Cx<float> dv = {0.f, 0.f};
-#pragma unroll
-                for (int g = 0; g < MM::NG; ++g) {
-                    const Cx<float> vg = ldc(MM::diag(g), n0 + e);
-                    const float cg = cs[(v * P + p) * NC + MM::ND + g];
-                    dv.re = fmaf(cg, vg.re, dv.re);
-                    dv.im = fmaf(cg, vg.im, dv.im);
+                for (int e = 0; e < E; ++e) {
+                    Kr[e] = (q == 0) ? a[e] : fmaf(cq[q], a[e], Kr[e]);
+                    Ki[e] = (q == 0) ? b[e] : fmaf(cq[q], b[e], Ki[e]);
                 }
-                Kr[e] = fmaf(dv.re, ur[e], fmaf(-dv.im, ui[e], Kr[e]));
-                Ki[e] = fmaf(dv.re, ui[e], fmaf(dv.im, ur[e], Ki[e]));
             }
-        }
+            if constexpr (MM::kOwnTerms || (T::NGM < MM::NG)) {  // terms that need the stage input itself
+                float a[8], b[8], c2[8], d2[8];
+                gqtc::tmem_ld8(t_ahi + n0, a);
+                gqtc::tmem_ld8(t_ahi + N + n0, b);
+                gqtc::tmem_ld8(t_alo + n0, c2);
+                gqtc::tmem_ld8(t_alo + N + n0, d2);
+                gqtc::tmem_wait_ld();
 #pragma unroll
-        for (int e = 0; e < E; ++e) kbuf[(p * N + j) * LDK + n0 + e] = {Kr[e], Ki[e]};
-        __syncthreads();  // K complete
+                for (int e = 0; e < E; ++e) {
+                    ur[e] = a[e] + c2[e];
+                    ui[e] = b[e] + d2[e];
+                }
+            }
+            if constexpr (T::NGM < MM::NG) {  // diagonal terms in the epilogue: K += (sum_g c_g v_g[n]) u[n][j]
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    Cx<float> dv = {0.f, 0.f};
+#pragma unroll
+                    for (int g = 0; g < MM::NG; ++g) {
+                        const Cx<float> vg = ldc(MM::diag(g), n0 + e);
+                        const float cg = cs[(v * P + p) * NC + MM::ND + g];
+                        dv.re = fmaf(cg, vg.re, dv.re);
+                        dv.im = fmaf(cg, vg.im, dv.im);
+                    }
+                    Kr[e] = fmaf(dv.re, ur[e], fmaf(-dv.im, ui[e], Kr[e]));
+                    Ki[e] = fmaf(dv.re, ui[e], fmaf(dv.im, ur[e], Ki[e]));
+                }
+            }
+            // K[n][j] for the rows n of this thread goes to the CTA that reads row j of K transposed
+            const int kdst = j / NH;
+            Cx<float>* const kb = (T::CL > 1 && kdst != crank) ? kbuf_peer : kbuf;
+#pragma unroll
+            for (int e = 0; e < E; ++e) kb[(p * NH + (j - kdst * NH)) * LDK + n0 + e] = {Kr[e], Ki[e]};
+        }  // !bad
+        if constexpr (T::CL > 1) {
+            if (tid == 0 && bad) *flag_peer = 1u;
+            gqtc::cluster_sync();  // K complete in both CTAs; a failure is known to both
+            if (bad || *reinterpret_cast<volatile uint32_t*>(fail_flag) != 0u) return false;
+        } else {
+            __syncthreads();  // K complete
+        }
 #pragma unroll
         for (int e = 0; e < E; ++e) {
-            const int n = n0 + e;
-            const Cx<float> kt = kbuf[(p * N + n) * LDK + j];  // K[j][n]
+            const Cx<float> kt = kbuf[(p * NH + (n0 - nb + e)) * LDK + j];  // K[j][n], n = n0 + e
             kre[e] = Ki[e] + kt.im;                             // -i (K[n][j] - conj(K[j][n]))
             kim[e] = kt.re - Kr[e];
         }
@@ -362,28 +447,48 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
         return true;
     };
 
-    const double dt = d.dt, dt2d = dt * 0.5;
     const float h = (float)dt, h2 = (float)dt2d;
     const Coef<float> h6 = Coef<float>::make(dt / 6.0);
     double osum_re = 0.0, osum_im = 0.0;
-    // Sum of (re, im) over the threads of point p, valid in its lead thread: over the N columns (lanes
-    // p*N .. p*N+N-1 of a warp), then over the H row blocks through shared memory. Uniform over the CTA.
+    // Sum of (re, im) over the threads of point p, valid in its lead thread (of cluster rank 0): over
+    // the point's columns in a warp (lanes p*N .. of at most 32), then over the row blocks and warps
+    // through shared memory, then over the cluster. Uniform over the CTA (the cluster); the barrier
+    // in front keeps a previous call's reads of the sums apart from this call's writes.
     auto point_sum = [&](double& re, double& im) {
+        if constexpr (T::CL > 1) {
+            gqtc::cluster_sync();
+        } else {
+            __syncthreads();
+        }
+        constexpr int W = N < 32 ? N : 32;  // columns of the point in one warp
 #pragma unroll
-        for (int off = N / 2; off > 0; off >>= 1) {
+        for (int off = W / 2; off > 0; off >>= 1) {
             re += __shfl_xor_sync(0xffffffffu, re, off);
             im += __shfl_xor_sync(0xffffffffu, im, off);
         }
-        if (j == 0) {
-            red[(0 * T::H + hh) * P + p] = re;
-            red[(1 * T::H + hh) * P + p] = im;
+        constexpr int NR = T::H * T::CG;  // partial sums of a point: row blocks x warps of columns
+        if (j % W == 0) {
+            red[(0 * NR + hh * T::CG + j / W) * P + p] = re;
+            red[(1 * NR + hh * T::CG + j / W) * P + p] = im;
         }
         __syncthreads();
         if (lead) {
             re = im = 0.0;
-            for (int g = 0; g < T::H; ++g) {
-                re += red[(0 * T::H + g) * P + p];
-                im += red[(1 * T::H + g) * P + p];
+            for (int g = 0; g < NR; ++g) {
+                re += red[(0 * NR + g) * P + p];
+                im += red[(1 * NR + g) * P + p];
+            }
+        }
+        if constexpr (T::CL > 1) {
+            constexpr int PS = 2 * T::H * T::CG * P;  // the partner's sums
+            if (lead && crank == 1) {
+                red_peer[PS + 2 * p] = re;
+                red_peer[PS + 2 * p + 1] = im;
+            }
+            gqtc::cluster_sync();
+            if (lead && crank == 0) {
+                re += red[PS + 2 * p];
+                im += red[PS + 2 * p + 1];
             }
         }
     };
@@ -400,19 +505,22 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
 
     // Evaluations it = 4 n + s (step n, stage s). Stage times: s = 0 at the previous step's end
     // (t_in + 0 for n = 0), s = 1, 2 at t_mid = (n + 1/2) dt, s = 3 at t_mid + dt/2 - the times and
-    // roundings of gqfixed::RK4. Coefficients change at it = 0 and at s = 1, 3 (version cv).
+    // roundings of gqfixed::RK4, whose coefficients come from the table (block step / KB). The next
+    // block's table is filled during the MMA of stage 1 of a block's last step.
     bool failed = false;
     {
         float kre[E], kim[E];
 #pragma unroll
         for (int e = 0; e < E; ++e) kre[e] = kim[e] = 0.f;
-        int cv = 0;
-        coef(d.t_in + 0.0, cv);
+        fill_table(0);
         write_stage(0.f, kre, kim, 0);
         const int total = 4 * d.num_steps;
         for (int it = 0; it < total; ++it) {
             const int step = it >> 2, s = it & 3;
-            if (!eval(kre, kim, it & 1, cv)) {
+            const int sb = step % T::KB;
+            const int ver = ((step / T::KB) & 1) * T::TS + 3 * sb + (s == 0 ? 0 : (s == 3 ? 2 : 1));
+            const int fill = (s == 1 && sb == T::KB - 1) ? step / T::KB + 1 : -1;
+            if (!eval(kre, kim, it & 1, ver, fill)) {
                 failed = true;
                 break;
             }
@@ -435,7 +543,7 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
                         osum_re = s_re;
                         osum_im = s_im;
                         point_sum(tre, tim);
-                        if (lead && active && sample < d.num_trace) {
+                        if (lead && active && crank == 0 && sample < d.num_trace) {
                             float* tr = static_cast<float*>(d.trace) + ((size_t)local * d.num_trace + sample) * 2;
                             tr[0] = (float)tre;
                             tr[1] = (float)tim;
@@ -449,24 +557,17 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
                 for (int e = 0; e < E; ++e) kre[e] = kim[e] = 0.f;
                 write_stage(0.f, kre, kim, nslot);  // input of the next step's k1 (same time)
             } else {
-                const double t_mid = ((double)step + 0.5) * dt;
                 if (s == 0) {
 #pragma unroll
                     for (int e = 0; e < E; ++e) {
                         are[e] = kre[e];
                         aim[e] = kim[e];
                     }
-                    cv ^= 1;
-                    coef(d.t_in + t_mid, cv);
                 } else {
 #pragma unroll
                     for (int e = 0; e < E; ++e) {
                         are[e] = fmaf(2.f, kre[e], are[e]);
                         aim[e] = fmaf(2.f, kim[e], aim[e]);
-                    }
-                    if (s == 2) {
-                        cv ^= 1;
-                        coef(d.t_in + (t_mid + dt2d), cv);
                     }
                 }
                 write_stage(s == 2 ? h : h2, kre, kim, nslot);
@@ -478,7 +579,7 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
     if (failed) {
         // the MMA of the last phase did not signal: wait once more (bounded), mark the tile's outputs
         gqtc::mbar_wait_bounded(bar, phase, kMaxPolls);
-        if (active && lead) {
+        if (active && lead && crank == 0) {
             const int width = (OUT == GQIS_OUT_FINAL_STATE) ? MM::S : 2;
             for (int i = 0; i < width; ++i) out[(size_t)local * width + i] = __int_as_float(0x7fc00000);
         }
@@ -500,7 +601,7 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
     } else {
         if constexpr (OUT == GQIS_OUT_FINAL) observe();
         point_sum(osum_re, osum_im);
-        if (lead && active) {
+        if (lead && active && crank == 0) {
             double sr = osum_re, si = osum_im;
             if constexpr (OUT == GQIS_OUT_MEAN) {
                 const double inv = 1.0 / (double)(d.num_steps - d.warmup_steps);
@@ -513,6 +614,7 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
     }
     gqtc::fence_before_sync();
     __syncthreads();
+    if constexpr (T::CL > 1) gqtc::cluster_sync();  // no access to the partner's memory after this
     if (warp == 0) {
         gqtc::fence_after_sync();
         gqtc::tmem_dealloc(tbase, T::TMEM_COLS);

@@ -48,11 +48,13 @@ using Model = GQ_MODEL;
 using Form = GQ_FORM;
 
 #if GQ_MATRIX == 2
-// Density-matrix form on the tensor cores (gqis_matrix_tc.cuh): one CTA per tile of 128 / N points.
+// Density-matrix form on the tensor cores (gqis_matrix_tc.cuh): one CTA (N <= 32) or one cluster of
+// two CTAs (N = 64) per tile of 128 / N points.
 constexpr auto kKernel = gqmatrix_tc::matrix_tc_kernel<Model, GQ_OUT, GQ_TRACE>;
 constexpr int kBlock = gqmatrix_tc::TcShape<Model>::THREADS;
 constexpr size_t kSmem = gqmatrix_tc::TcShape<Model>::SMEM;
 constexpr int kPointsPerCta = gqmatrix_tc::TcShape<Model>::P;
+constexpr int kCluster = gqmatrix_tc::TcShape<Model>::CL;
 static_assert(Form::id == GQIS_FORM_FP32, "the tensor-core form is an FP32 form");
 #elif GQ_MATRIX
 // Density-matrix form (gqis_matrix.cuh, included by the generated source): one CTA per point.
@@ -60,6 +62,7 @@ constexpr auto kKernel = gqmatrix::matrix_rk4_kernel<Model, Form, GQ_OUT, GQ_TRA
 constexpr int kBlock = Model::THREADS;
 constexpr size_t kSmem = gqmatrix::smem_bytes<Model, typename Form::real>();
 constexpr int kPointsPerCta = 1;
+constexpr int kCluster = 1;
 static_assert(std::is_same<typename Model::real, typename Form::real>::value, "model data type");
 #elif GQ_ADAPTIVE
 constexpr auto kKernel = gqadaptive::sweep_adaptive_kernel<GQ_SOLVER, Model, Form, GQ_OUT, GQ_TRACE>;
@@ -149,9 +152,25 @@ __attribute__((visibility("default"))) int gqis_sweep_launch(const gqis_sweep_de
     if (kSmem > 48 * 1024 &&
         (e = cudaFuncSetAttribute(kKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem)) != cudaSuccess)
         return cuda_fail(e, "cudaFuncSetAttribute(max dynamic shared memory)");
-    const int64_t grid = (d->point_count + kPointsPerCta - 1) / kPointsPerCta;
+    const int64_t grid = (d->point_count + kPointsPerCta - 1) / kPointsPerCta * kCluster;
     if (grid > 0x7fffffffLL) return fail(GQIS_ERR_TOO_LARGE, "too many points for one launch");
-    kKernel<<<(unsigned)grid, kBlock, kSmem, st>>>(*d);
+    if (kCluster > 1) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)grid, 1, 1);
+        cfg.blockDim = dim3(kBlock, 1, 1);
+        cfg.dynamicSmemBytes = kSmem;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = kCluster;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        if ((e = cudaLaunchKernelEx(&cfg, kKernel, *d)) != cudaSuccess) return cuda_fail(e, "cluster launch");
+    } else {
+        kKernel<<<(unsigned)grid, kBlock, kSmem, st>>>(*d);
+    }
 #elif GQ_ADAPTIVE
     // Persistent grid: every resident CTA slot of the device, lanes refill themselves.
     int dev = 0, sms = 0, ctas = 0;

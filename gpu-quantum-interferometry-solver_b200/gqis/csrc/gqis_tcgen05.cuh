@@ -2,8 +2,9 @@
 // mbarrier instructions used by gqis_matrix_tc.cuh, written as inline PTX (PTX ISA 8.7+).
 //
 // Only the forms this engine needs: cta_group::1, kind::tf32 with A in tensor memory and B in
-// shared memory (K-major, no swizzle), 32x32b tensor-memory loads/stores, and mbarrier waits
-// that give up after a bounded number of polls.
+// shared memory (K-major, no swizzle), 32x32b tensor-memory loads/stores, mbarrier waits that give
+// up after a bounded number of polls, and the cluster barrier / distributed-shared-memory mapping
+// of two-CTA clusters (plain stores; no TMA, no multicast).
 #pragma once
 
 #include <stdint.h>
@@ -104,6 +105,25 @@ __device__ __forceinline__ void tmem_st8(uint32_t taddr, const float (&v)[8]) {
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// ---- thread-block clusters: rank in the cluster, the cluster-wide barrier (every thread of every CTA of
+// the cluster arrives; shared-memory writes before it, local or remote, are visible after it; the
+// non-.aligned forms, so a warp need not be converged there), and the generic address of the same
+// shared-memory location in another CTA of the cluster (mapa).
+__device__ __forceinline__ uint32_t cluster_ctarank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ void cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
+}
+template <class T>
+__device__ __forceinline__ T* cluster_peer(T* p, uint32_t rank) {
+    uint64_t out;
+    asm volatile("mapa.u64 %0, %1, %2;" : "=l"(out) : "l"(reinterpret_cast<uint64_t>(p)), "r"(rank));
+    return reinterpret_cast<T*>(out);
+}
 
 // Round to TF32 (nearest, ties away from zero); the result is an FP32 number with 10 mantissa bits.
 __device__ __forceinline__ float to_tf32(float x) {

@@ -455,7 +455,31 @@ def emit_matrix_model(mm: MatrixModel, form: str, uses_rho0_values: bool, tensor
 
 
 OUTPUT_IDS = {"mean": 0, "final": 1, "final_rho": 2}
-TENSOR_DIMS = (8, 16, 32)
+TENSOR_DIMS = (8, 16, 32, 64)
+SMEM_LIMIT = 232448  # shared memory of one CTA on sm_100a (bytes)
+
+
+def tensor_core_shape(mm: MatrixModel):
+    """(cluster CTAs, rows per CTA, MMA columns, shared-memory bytes) of the tcgen05 kernel for this model,
+    the TcShape of csrc/gqis_matrix_tc.cuh (a generated module asserts that the sizes agree)."""
+    Np = mm.Np
+    cl = 2 if Np == 64 else 1
+    nh = Np // cl
+    P, E = 128 // Np, 8
+    H = nh // E
+    terms = 1 + mm.num_dense + (mm.num_diag if diag_in_mma(mm) else 0)
+    nmma = 2 * nh * terms
+    kdim = 2 * Np
+    nc = max(1, len(mm.coef_exprs))
+    b = nmma * kdim * 4
+    k = P * nh * (Np + 1) * 8
+    x = P * H * E * Np * 8 if cl > 1 else 0
+    rd = 2 * P * Np * 4
+    cs = 2 * 24 * P * nc * 4  # coefficient table: 2 buffers x 3 stage times x 8 steps
+    cg = Np // 32 if Np > 32 else 1
+    off_red = -(-(2 * b + k + x + rd + cs) // 8) * 8
+    needed = off_red + 2 * H * cg * P * 8 + 2 * P * 8 + 64
+    return cl, nh, nmma, needed
 
 
 def tensor_core_blockers(mm: MatrixModel, form: str):
@@ -465,9 +489,14 @@ def tensor_core_blockers(mm: MatrixModel, form: str):
         out.append("the tensor-core form is an FP32 form (precision='fp32')")
     if mm.Np not in TENSOR_DIMS:
         out.append(f"padded dimension {mm.Np} is not one of {TENSOR_DIMS}")
-    elif 2 * mm.Np * (1 + mm.num_dense + (mm.num_diag if diag_in_mma(mm) else 0)) > 256:
-        out.append(f"{mm.num_dense + mm.num_diag} coefficient operator terms exceed one MMA "
-                   "(2 N (1 + terms) <= 256)")
+    else:
+        _, nh, nmma, smem = tensor_core_shape(mm)
+        if nmma > 256:
+            out.append(f"{mm.num_dense + mm.num_diag} coefficient operator terms exceed one MMA "
+                       f"(2 x {nh} rows x (1 + terms) <= 256)")
+        elif smem > SMEM_LIMIT:
+            out.append(f"{mm.num_dense} dense coefficient operators need {smem} bytes of shared memory per CTA "
+                       f"(at most {SMEM_LIMIT})")
     if any(src != dst and src // mm.Np != src % mm.Np for dst, src, _, _ in mm.jumps):
         out.append("a jump term moves a coherence to another element (only populations may feed other elements)")
     elif mm.Np in TENSOR_DIMS:
@@ -507,8 +536,8 @@ def module_source(mm: MatrixModel, form: str, output_mode: str, uses_rho0_values
         f"#define GQ_TRACE {1 if trace else 0}",
         f"#define GQ_MODEL_HASH 0x{model_hash:016x}ULL",
         '#include "gqis_module.cuh"',
-        "",
-    ])
+    ] + ([f"static_assert(gqmatrix_tc::TcShape<gqmodel::MM>::NEEDED == {tensor_core_shape(mm)[3]}, "
+          '"shared-memory size of matrix_form.tensor_core_shape");'] if tensor_cores else []) + [""])
 
 
 def flops_per_point_step(mm: MatrixModel):

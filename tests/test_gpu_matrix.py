@@ -104,9 +104,11 @@ def test_tensor_core_form_vs_oracle(N):
 
 
 @pytest.mark.gpu
-def test_tensor_core_form_final_rho():
+@pytest.mark.parametrize("N", [16, 64])
+def test_tensor_core_form_final_rho(N):
+    """The final state in the reduced layout; at N = 64 each CTA of the cluster writes its half of the rows."""
     import gqis
-    w, args, kwargs = hilbert_model(16)
+    w, args, kwargs = hilbert_model(N)
     got = gqis.mesolve_2D(*args, **kwargs, precision="fp32", rhs_form="matrix_tc", output_mode="final_rho")
     ref = _oracle(w, kwargs, output_mode="final_rho")
     assert got.shape == ref.shape
@@ -153,3 +155,19 @@ def test_matrix_forms_record_the_observable_trace(form, rhs_form, tol):
     np.testing.assert_allclose(got_t, ref_t, rtol=1e-6)
     assert float(np.max(np.abs(got_tr - ref_tr))) <= tol
     assert float(np.max(np.abs(got_map - ref_map))) <= tol
+
+
+@pytest.mark.gpu
+def test_two_cta_tensor_core_kernel_records_the_trace():
+    """N = 64 runs on a cluster of two CTAs per tile whose point sums meet through distributed shared
+    memory: its observable trace (every 9th step) against the FP64 CUDA-core matrix form."""
+    import gqis
+    w, args, kwargs = hilbert_model(64)
+    trace = dict(kwargs, return_time_trace=True, time_trace_every=9)
+    ref_map, ref_tr, ref_t = gqis.mesolve_2D(*args, **trace, fp64=True, rhs_form="matrix")
+    got_map, got_tr, got_t = gqis.mesolve_2D(*args, **trace, precision="fp32", rhs_form="matrix_tc")
+    assert got_tr.shape == ref_tr.shape and got_tr.shape[2] == 12
+    np.testing.assert_allclose(got_t, ref_t, rtol=1e-6)
+    assert float(np.max(np.abs(ref_tr))) > 1e-4  # the top level's population grows to ~1e-3 by t = 5
+    assert float(np.max(np.abs(got_tr - ref_tr))) <= 5e-6
+    assert float(np.max(np.abs(got_map - ref_map))) <= 5e-6

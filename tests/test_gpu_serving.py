@@ -73,13 +73,15 @@ def test_fit_requests_in_the_server_match_the_adjoint_alone():
 
 
 @pytest.mark.gpu
-def test_tensor_core_request_is_the_same_in_chunks_that_split_tiles():
-    """The tensor-core kernel packs 128 / N points per MMA tile; a chunk size that is not a multiple
-    of the tile moves every point to another row of another tile, and the result must not change."""
+@pytest.mark.parametrize("N", [16, 64])
+def test_tensor_core_request_is_the_same_in_chunks_that_split_tiles(N):
+    """The tensor-core kernel packs 128 / N points per MMA tile (at N = 64 a tile spans a cluster of
+    two CTAs); a chunk size that is not a multiple of the tile moves every point to another row of
+    another tile, and the result must not change."""
     import gqis
     from gqis.serving import SweepServer
     from test_support_calls import hilbert_model
-    _, args, kwargs = hilbert_model(16, side=(12, 9))
+    _, args, kwargs = hilbert_model(N, side=(12, 9) if N == 16 else (5, 3))
     alone = gqis.mesolve_2D(*args, **kwargs, precision="fp32", rhs_form="matrix_tc")
     with SweepServer(streams=3, chunk_points=13, max_inflight=4) as srv:
         out = srv.submit("mesolve_2D", *args, **kwargs, precision="fp32", rhs_form="matrix_tc").result(300)

@@ -128,3 +128,24 @@ def test_tensor_core_jump_lists_of_a_dephased_qubit():
     assert any(e == 1 and a == 1 for e, a, c, r in col1)               # population (1, 1) from itself
     assert any(e == 0 and a == 1 for e, a, c, r in lists[0][0])        # (0, 0) fed by rho_11 (relaxation)
     assert matrix_form.tensor_core_blockers(mm, "fp32") == []
+
+
+def test_tensor_core_shape_of_the_two_cta_kernel():
+    """N = 64 splits each tile's rows over a cluster of two CTAs: half the B columns per CTA, and the
+    shared memory (B, transposed K, exchange buffer) must fit one CTA; more dense operators do not."""
+    from types import SimpleNamespace
+    import numpy as np
+
+    def fake(Np, dense, diag):
+        return SimpleNamespace(Np=Np, num_dense=dense, num_diag=diag, coef_exprs=[0] * (dense + diag),
+                               jumps=[], wjump=np.zeros((Np, Np)))
+    cl, nh, nmma, smem = matrix_form.tensor_core_shape(fake(64, 1, 1))
+    assert (cl, nh, nmma) == (2, 32, 128) and smem <= matrix_form.SMEM_LIMIT
+    assert matrix_form.tensor_core_blockers(fake(64, 1, 1), "fp32") == []
+    assert matrix_form.tensor_core_shape(fake(32, 1, 1))[:3] == (1, 32, 128)  # diagonal in the epilogue
+    assert matrix_form.tensor_core_shape(fake(16, 1, 1))[:3] == (1, 16, 96)   # diagonal on the MMA
+    blocked = matrix_form.tensor_core_blockers(fake(64, 2, 1), "fp32")
+    assert len(blocked) == 1 and "shared memory" in blocked[0]
+    assert matrix_form.tensor_core_blockers(fake(32, 3, 1), "fp32") == []  # 2 x 32 x 4 = 256 columns
+    assert "exceed one MMA" in matrix_form.tensor_core_blockers(fake(32, 4, 1), "fp32")[0]
+    assert "padded dimension 48" in matrix_form.tensor_core_blockers(fake(48, 1, 1), "fp32")[0]

@@ -39,7 +39,7 @@ def serving_model(N, side):
 
 
 MATRIX_DIMS = (16, 32, 64)
-TENSOR_DIMS = (8, 16, 32)
+TENSOR_DIMS = (8, 16, 32, 64)
 
 
 def hilbert_model(N, side=(4, 3), steps=100, duration=5.0):
@@ -61,8 +61,14 @@ def matrix_calls():
     for N in TENSOR_DIMS:
         _, args, kwargs = hilbert_model(N)
         out.append(("mesolve_2D", args, dict(kwargs, precision="fp32", rhs_form="matrix_tc")))
+    for N in (16, 64):
+        _, args, kwargs = hilbert_model(N)
+        out.append(("mesolve_2D", args, dict(kwargs, precision="fp32", rhs_form="matrix_tc", output_mode="final_rho")))
+    _, args, kwargs = hilbert_model(64)  # the two-CTA tensor-core kernel's trace against the FP64 matrix form
+    trace64 = dict(kwargs, return_time_trace=True, time_trace_every=9)
+    out.append(("mesolve_2D", args, dict(trace64, fp64=True, rhs_form="matrix")))
+    out.append(("mesolve_2D", args, dict(trace64, precision="fp32", rhs_form="matrix_tc")))
     _, args, kwargs = hilbert_model(16)
-    out.append(("mesolve_2D", args, dict(kwargs, precision="fp32", rhs_form="matrix_tc", output_mode="final_rho")))
     out.append(("mesolve_2D", args, dict(kwargs, fp64=True, rhs_form="matrix", output_mode="final_rho")))
     rho0 = np.zeros((4, 3, 16 * 16 - 1))
     out.append(("mesolve_2D", args, dict(kwargs, fp64=True, rhs_form="matrix", output_mode="final_rho",
