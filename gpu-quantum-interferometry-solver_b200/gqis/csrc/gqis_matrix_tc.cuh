@@ -74,13 +74,13 @@ struct TcShape {
     static constexpr int COLS_USED = NMMA + 2 * KDIM;
     static constexpr int TMEM_COLS = COLS_USED <= 32 ? 32 : COLS_USED <= 64 ? 64 : COLS_USED <= 128 ? 128
                                    : COLS_USED <= 256 ? 256 : 512;
-    static constexpr int LDK = N + 1;         // padded column stride of the K buffer
+    static constexpr int LDK = N + 2;         // padded column stride of the K buffer (16-byte rows, no conflicts)
     // shared memory layout (bytes)
     static constexpr size_t B_BYTES = (size_t)NMMA * KDIM * 4;
     static constexpr size_t OFF_BHI = 0, OFF_BLO = B_BYTES;
     static constexpr size_t OFF_K = 2 * B_BYTES;
     static constexpr size_t K_BYTES = (size_t)P * NH * LDK * 8;  // K[j][n] for the CTA's rows n, every j
-    static constexpr size_t OFF_X = OFF_K + K_BYTES;            // [P][H][E][N] the partner's stage input
+    static constexpr size_t OFF_X = OFF_K + K_BYTES;            // [P][H][E/2][N] x 2 the partner's stage input
     static constexpr size_t X_BYTES = CL > 1 ? (size_t)P * H * E * N * 8 : 0;
     static constexpr size_t OFF_RD = OFF_X + X_BYTES;           // [2][P*N] populations of the stage input
     static constexpr size_t RD_BYTES = 2 * (size_t)P * N * 4;
@@ -185,18 +185,10 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
     gqtc::fence_before_sync();
     __syncthreads();
     gqtc::fence_after_sync();
-    // the partner CTA's buffers (distributed shared memory); both CTAs run before either writes there
-    Cx<float>* kbuf_peer = kbuf;
-    float2* xbuf_peer = xbuf;
-    double* red_peer = red;
-    uint32_t* flag_peer = fail_flag;
-    if constexpr (T::CL > 1) {
-        kbuf_peer = gqtc::cluster_peer(kbuf, (uint32_t)(crank ^ 1));
-        xbuf_peer = gqtc::cluster_peer(xbuf, (uint32_t)(crank ^ 1));
-        red_peer = gqtc::cluster_peer(red, (uint32_t)(crank ^ 1));
-        flag_peer = gqtc::cluster_peer(fail_flag, (uint32_t)(crank ^ 1));
-        gqtc::cluster_sync();
-    }
+    // The partner CTA's buffers (distributed shared memory) are mapped where they are used (one mapa
+    // each, which keeps no address live across the loop); both CTAs run before either writes there.
+    const uint32_t peer = (uint32_t)(crank ^ 1);
+    if constexpr (T::CL > 1) gqtc::cluster_sync();
     const uint32_t tbase = *tslot;
     const uint32_t t_d = tbase + T::COL_D + lane_base;
     const uint32_t t_ahi = tbase + T::COL_AHI + lane_base;
@@ -276,6 +268,7 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
     // also into the partner's exchange buffer (its rows of A are this CTA's rows)
     auto write_stage = [&](float s, const float (&kre)[E], const float (&kim)[E], int slot) {
         float hr[E], hi_[E], lr[E], li[E];
+        float pr = 0.f, pi = 0.f;  // the previous row's stage input
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             const float ur = fmaf(s, kre[e], yre[e]), ui = fmaf(s, kim[e], yim[e]);
@@ -284,7 +277,14 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
             lr[e] = ur - hr[e];  // |lo| <= 2^-11 |u|; its TF32 read loses at most 2^-21 |u|
             li[e] = ui - hi_[e];
             if (n0 + e == j) rdiag[slot * P * N + p * N + j] = ur;
-            if constexpr (T::CL > 1) xbuf_peer[((p * H + hh) * E + e) * N + j] = make_float2(ur, ui);
+            if constexpr (T::CL > 1) {  // rows e - 1, e as one 16-byte remote store
+                if (e & 1)
+                    gqtc::st_cluster_v4(gqtc::cluster_peer_u32(xbuf, peer) +
+                                            (uint32_t)((((p * H + hh) * (E / 2) + e / 2) * N + j) * 16),
+                                        pr, pi, ur, ui);
+            }
+            pr = ur;
+            pi = ui;
         }
         gqtc::tmem_st8(t_ahi + n0, hr);
         gqtc::tmem_st8(t_ahi + N + n0, hi_);
@@ -300,20 +300,39 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
         if constexpr (T::CL > 1) {
             gqtc::cluster_sync();  // the partner's half of the stage input is in xbuf
             const int mb = (crank ^ 1) * NH + hh * E;
-            float hr[E], hi_[E], lr[E], li[E];
+            const float4* xs = reinterpret_cast<const float4*>(xbuf) + (p * H + hh) * (E / 2) * N + j;
+            float ur[E], ui[E];
 #pragma unroll
-            for (int e = 0; e < E; ++e) {
-                const float2 u = xbuf[((p * H + hh) * E + e) * N + j];
-                hr[e] = tf32_round(u.x);
-                hi_[e] = tf32_round(u.y);
-                lr[e] = u.x - hr[e];
-                li[e] = u.y - hi_[e];
-                if (mb + e == j) rdiag[slot * P * N + p * N + j] = u.x;
+            for (int e2 = 0; e2 < E / 2; ++e2) {
+                const float4 u = xs[e2 * N];
+                ur[2 * e2] = u.x;
+                ui[2 * e2] = u.y;
+                ur[2 * e2 + 1] = u.z;
+                ui[2 * e2 + 1] = u.w;
             }
-            gqtc::tmem_st8(t_ahi + mb, hr);
-            gqtc::tmem_st8(t_ahi + N + mb, hi_);
-            gqtc::tmem_st8(t_alo + mb, lr);
-            gqtc::tmem_st8(t_alo + N + mb, li);
+#pragma unroll
+            for (int e = 0; e < E; ++e)
+                if (mb + e == j) rdiag[slot * P * N + p * N + j] = ur[e];
+            {
+                float hv[E], lv[E];
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    hv[e] = tf32_round(ur[e]);
+                    lv[e] = ur[e] - hv[e];
+                }
+                gqtc::tmem_st8(t_ahi + mb, hv);
+                gqtc::tmem_st8(t_alo + mb, lv);
+            }
+            {
+                float hv[E], lv[E];
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    hv[e] = tf32_round(ui[e]);
+                    lv[e] = ui[e] - hv[e];
+                }
+                gqtc::tmem_st8(t_ahi + N + mb, hv);
+                gqtc::tmem_st8(t_alo + N + mb, lv);
+            }
         }
         gqtc::tmem_wait_st();
         gqtc::fence_before_sync();
@@ -387,13 +406,22 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
                 }
             }
             // K[n][j] for the rows n of this thread goes to the CTA that reads row j of K transposed
+            // (16-byte stores: LDK even, n0 a multiple of 8)
             const int kdst = j / NH;
-            Cx<float>* const kb = (T::CL > 1 && kdst != crank) ? kbuf_peer : kbuf;
+            const int kidx = (p * NH + (j - kdst * NH)) * LDK + n0;
+            if constexpr (T::CL > 1) {
+                const uint32_t ka = (kdst != crank ? gqtc::cluster_peer_u32(kbuf, peer) : gqtc::smem_u32(kbuf)) +
+                                    (uint32_t)kidx * 8u;
 #pragma unroll
-            for (int e = 0; e < E; ++e) kb[(p * NH + (j - kdst * NH)) * LDK + n0 + e] = {Kr[e], Ki[e]};
+                for (int e = 0; e < E; e += 2) gqtc::st_cluster_v4(ka + 8u * e, Kr[e], Ki[e], Kr[e + 1], Ki[e + 1]);
+            } else {
+                float4* const kb = reinterpret_cast<float4*>(kbuf + kidx);
+#pragma unroll
+                for (int e = 0; e < E; e += 2) kb[e / 2] = make_float4(Kr[e], Ki[e], Kr[e + 1], Ki[e + 1]);
+            }
         }  // !bad
         if constexpr (T::CL > 1) {
-            if (tid == 0 && bad) *flag_peer = 1u;
+            if (tid == 0 && bad) *gqtc::cluster_peer(fail_flag, peer) = 1u;
             gqtc::cluster_sync();  // K complete in both CTAs; a failure is known to both
             if (bad || *reinterpret_cast<volatile uint32_t*>(fail_flag) != 0u) return false;
         } else {
@@ -482,6 +510,7 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
         if constexpr (T::CL > 1) {
             constexpr int PS = 2 * T::H * T::CG * P;  // the partner's sums
             if (lead && crank == 1) {
+                double* const red_peer = gqtc::cluster_peer(red, peer);
                 red_peer[PS + 2 * p] = re;
                 red_peer[PS + 2 * p + 1] = im;
             }

@@ -124,6 +124,17 @@ __device__ __forceinline__ T* cluster_peer(T* p, uint32_t rank) {
     asm volatile("mapa.u64 %0, %1, %2;" : "=l"(out) : "l"(reinterpret_cast<uint64_t>(p)), "r"(rank));
     return reinterpret_cast<T*>(out);
 }
+// shared::cluster address of the same location in CTA `rank` (a CTA's own shared::cta addresses are
+// valid shared::cluster addresses of itself), and a 16-byte store there
+__device__ __forceinline__ uint32_t cluster_peer_u32(const void* p, uint32_t rank) {
+    uint32_t out;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(out) : "r"(smem_u32(p)), "r"(rank));
+    return out;
+}
+__device__ __forceinline__ void st_cluster_v4(uint32_t addr, float a, float b, float c, float d) {
+    asm volatile("st.shared::cluster.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "f"(a), "f"(b), "f"(c), "f"(d)
+                 : "memory");
+}
 
 // Round to TF32 (nearest, ties away from zero); the result is an FP32 number with 10 mantissa bits.
 __device__ __forceinline__ float to_tf32(float x) {

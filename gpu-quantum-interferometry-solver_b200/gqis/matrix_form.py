@@ -472,7 +472,7 @@ def tensor_core_shape(mm: MatrixModel):
     kdim = 2 * Np
     nc = max(1, len(mm.coef_exprs))
     b = nmma * kdim * 4
-    k = P * nh * (Np + 1) * 8
+    k = P * nh * (Np + 2) * 8
     x = P * H * E * Np * 8 if cl > 1 else 0
     rd = 2 * P * Np * 4
     cs = 2 * 24 * P * nc * 4  # coefficient table: 2 buffers x 3 stage times x 8 steps
