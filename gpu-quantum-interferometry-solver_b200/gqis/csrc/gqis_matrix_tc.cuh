@@ -54,7 +54,7 @@ constexpr uint32_t kMaxPolls = 1u << 20;  // mbarrier polls before a wait gives 
 template <class MM>
 struct TcShape {
     static constexpr int N = MM::N;
-    static constexpr int CL = N == 64 ? 2 : 1;  // CTAs per tile (cluster size)
+    static constexpr int CL = MM::TC_CL;      // CTAs per tile (cluster size, chosen by the model emitter)
     static constexpr int NH = N / CL;         // rows n of every column held by one CTA
     static constexpr int P = 128 / N;         // points per tile
     static constexpr int E = 8;               // rows of a column per thread
@@ -96,6 +96,7 @@ struct TcShape {
     static constexpr size_t FLOOR = 233472 / (MAX_CTAS + 1) + 1;
     static constexpr size_t SMEM = ((NEEDED > FLOOR ? NEEDED : FLOOR) + 1023) / 1024 * 1024;
     static_assert(N == 8 || N == 16 || N == 32 || N == 64, "tensor-core form: padded dimension 8, 16, 32 or 64");
+    static_assert(CL == 1 || CL == 2, "one or two CTAs per tile");
     static_assert(H >= 1 && NH % E == 0, "rows per thread");
     static_assert(NMMA % 16 == 0 && NMMA <= 256, "MMA N dimension");
     static_assert(COLS_USED <= 512, "tensor memory columns");

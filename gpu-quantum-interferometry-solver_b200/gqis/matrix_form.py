@@ -372,6 +372,7 @@ def _tensor_core_tables(mm: MatrixModel):
     static constexpr bool kOwnTerms = {'true' if own else 'false'};
     static constexpr bool kJumpsOnDiagonal = {'true' if on_diag else 'false'};
     static constexpr bool kDiagInMma = {'true' if diag_in_mma(mm) else 'false'};
+    static constexpr int TC_CL = {tensor_core_shape(mm)[0]};
     __device__ __forceinline__ static const int* tcj_count() {{ return mm_tcj_count; }}
     __device__ __forceinline__ static const int* tcj_e() {{ return mm_tcj_e; }}
     __device__ __forceinline__ static const int* tcj_a() {{ return mm_tcj_a; }}
@@ -457,13 +458,18 @@ def emit_matrix_model(mm: MatrixModel, form: str, uses_rho0_values: bool, tensor
 OUTPUT_IDS = {"mean": 0, "final": 1, "final_rho": 2}
 TENSOR_DIMS = (8, 16, 32, 64)
 SMEM_LIMIT = 232448  # shared memory of one CTA on sm_100a (bytes)
+# Padded dimension from which a tile is split over a cluster of two CTAs. Only N = 64 needs it (one
+# SM's registers cannot hold the tile); splitting N = 16 / 32 tiles as well, which would let two CTAs
+# share an SM, measured 2x slower (30 -> 67 ms, 146 -> 290 ms for 4096 points x 2000 steps): the two
+# cluster barriers and remote stores of every stage cost more than the overlap gains.
+TC_CLUSTER_FROM = 64
 
 
 def tensor_core_shape(mm: MatrixModel):
     """(cluster CTAs, rows per CTA, MMA columns, shared-memory bytes) of the tcgen05 kernel for this model,
     the TcShape of csrc/gqis_matrix_tc.cuh (a generated module asserts that the sizes agree)."""
     Np = mm.Np
-    cl = 2 if Np == 64 else 1
+    cl = 2 if Np >= TC_CLUSTER_FROM else 1
     nh = Np // cl
     P, E = 128 // Np, 8
     H = nh // E
