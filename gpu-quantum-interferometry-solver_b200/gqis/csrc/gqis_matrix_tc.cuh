@@ -16,7 +16,9 @@
 // rows n in [nb, nb + NH), nb = c NH, NH = N / 2, of every column, multiplies with the B columns of
 // its rows only, and both CTAs keep the whole stage input in A. Each stage the CTAs swap their
 // halves of the stage input and the parts of K the other one reads transposed through distributed
-// shared memory (plain remote stores, then the cluster barrier).
+// shared memory: st.async stores into the partner's buffer that count their bytes on the partner's
+// mbarrier (one per buffer), on which one thread of the receiving CTA waits (bounded); no cluster-wide
+// barrier inside the integration loop.
 //
 // One MMA chain gives every point's T_q rho at once; the epilogue forms K = sum_q c_q(t) T_q rho
 // with the point's FP64-evaluated coefficients (c_0 = 1), -i (K - K^dag) through a transposed
@@ -35,8 +37,10 @@
 // coherences, kOwnTerms); those and the diagonal terms done in the epilogue read the stage input
 // back from A (hi + lo).
 // One thread polls the MMA's mbarrier (bounded); the CTA meets it at a barrier. On give-up the
-// CTA (both CTAs of a cluster, which learn of it at their next cluster barrier) writes NaN outputs,
-// waits (bounded) for the MMA in flight, frees its tensor memory and returns.
+// CTA writes NaN outputs, waits (bounded) for the MMA in flight, frees its tensor memory and returns.
+// A CTA of a cluster instead stops using the tensor cores but keeps exchanging (zeros) to the end of
+// the loop, so its partner never waits in vain; the two tell each other at one cluster barrier after
+// the loop, and both write NaN. A CTA whose exchange wait gives up stops waiting altogether.
 #pragma once
 
 #include <type_traits>
@@ -82,13 +86,14 @@ struct TcShape {
     static constexpr size_t K_BYTES = (size_t)P * NH * LDK * 8;  // K[j][n] for the CTA's rows n, every j
     static constexpr size_t OFF_X = OFF_K + K_BYTES;            // [P][H][E/2][N] x 2 the partner's stage input
     static constexpr size_t X_BYTES = CL > 1 ? (size_t)P * H * E * N * 8 : 0;
+    static constexpr uint32_t KX_BYTES = (uint32_t)(P * NH * NH * 8);  // K entries the partner sends per stage
     static constexpr size_t OFF_RD = OFF_X + X_BYTES;           // [2][P*N] populations of the stage input
     static constexpr size_t RD_BYTES = 2 * (size_t)P * N * 4;
     static constexpr size_t OFF_CS = OFF_RD + RD_BYTES;         // [2][TS][P][NC] coefficient table
     static constexpr size_t CS_BYTES = 2 * (size_t)TS * P * NC * 4;
     static constexpr size_t OFF_RED = (OFF_CS + CS_BYTES + 7) / 8 * 8;
     static constexpr size_t RED_BYTES = 2 * (size_t)H * CG * P * 8 + 2 * (size_t)P * 8;  // + the partner's sums
-    static constexpr size_t OFF_MISC = OFF_RED + RED_BYTES;     // mbarrier, tensor-memory slot, failure flag
+    static constexpr size_t OFF_MISC = OFF_RED + RED_BYTES;     // mbarriers, tensor-memory slot, failure flag
     static constexpr size_t NEEDED = OFF_MISC + 64;
     // At most 512 / TMEM_COLS CTAs can hold tensor memory on one SM: pad the shared memory so that
     // no more CTAs fit (228 KB per SM, 1 KB reserved per CTA) and no allocation ever waits.
@@ -134,6 +139,8 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
     uint64_t* const bar = reinterpret_cast<uint64_t*>(gq_smem + T::OFF_MISC);
     uint32_t* const tslot = reinterpret_cast<uint32_t*>(gq_smem + T::OFF_MISC + 8);
     uint32_t* const fail_flag = reinterpret_cast<uint32_t*>(gq_smem + T::OFF_MISC + 12);  // set by the partner
+    uint64_t* const xbar = reinterpret_cast<uint64_t*>(gq_smem + T::OFF_MISC + 16);  // partner's stage input in
+    uint64_t* const kbar = reinterpret_cast<uint64_t*>(gq_smem + T::OFF_MISC + 24);  // partner's K entries in
 
     const int tid = threadIdx.x;
     const int r = tid & 127;
@@ -178,6 +185,10 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
     if (tid == 0) {
         gqtc::mbar_init(bar, 1);
         *fail_flag = 0u;
+        if constexpr (T::CL > 1) {
+            gqtc::mbar_init(xbar, 1);
+            gqtc::mbar_init(kbar, 1);
+        }
     }
     if (warp == 0) {
         gqtc::tmem_alloc(tslot, T::TMEM_COLS);
@@ -280,9 +291,9 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
             if (n0 + e == j) rdiag[slot * P * N + p * N + j] = ur;
             if constexpr (T::CL > 1) {  // rows e - 1, e as one 16-byte remote store
                 if (e & 1)
-                    gqtc::st_cluster_v4(gqtc::cluster_peer_u32(xbuf, peer) +
-                                            (uint32_t)((((p * H + hh) * (E / 2) + e / 2) * N + j) * 16),
-                                        pr, pi, ur, ui);
+                    gqtc::st_async_v4(gqtc::cluster_peer_u32(xbuf, peer) +
+                                          (uint32_t)((((p * H + hh) * (E / 2) + e / 2) * N + j) * 16),
+                                      pr, pi, ur, ui, gqtc::cluster_peer_u32(xbar, peer));
             }
             pr = ur;
             pi = ui;
@@ -293,13 +304,29 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
         gqtc::tmem_st8(t_alo + N + n0, li);
     };
 
-    uint32_t phase = 0;
+    uint32_t phase = 0, xphase = 0, kphase = 0;
+    bool failed = false;    // the tile's results are lost (uniform over the CTA)
+    bool mma_lost = false;  // an MMA wait gave up: that MMA may still be in flight
+    bool dead = false;      // an exchange wait gave up: no more waits (cluster CTAs)
+    // Waits (one thread, bounded) until the partner's bytes of this phase are in (expecting `bytes`).
+    auto exchange_wait = [&](uint64_t* xb, uint32_t& ph, uint32_t bytes) {
+        bool ok = true;
+        if (tid == 0 && !dead) {
+            gqtc::mbar_arrive_expect_tx(xb, bytes);
+            ok = gqtc::mbar_wait_bounded(xb, ph, kMaxPolls);
+        }
+        if (__syncthreads_or(!ok)) {
+            dead = true;
+            failed = true;
+        }
+        ph ^= 1u;
+    };
     // k = f(u) for the stage input in A with the coefficients of table entry v; false when the MMA wait
-    // gave up (uniform over the CTA and the cluster). While the MMA runs, the threads fill the
-    // coefficient table of block `fill` (if >= 0).
+    // gave up (one CTA; uniform over it). While the MMA runs, the threads fill the coefficient table of
+    // block `fill` (if >= 0).
     auto eval = [&](float (&kre)[E], float (&kim)[E], int slot, int v, int fill) -> bool {
         if constexpr (T::CL > 1) {
-            gqtc::cluster_sync();  // the partner's half of the stage input is in xbuf
+            exchange_wait(xbar, xphase, (uint32_t)T::X_BYTES);  // the partner's half of the stage input
             const int mb = (crank ^ 1) * NH + hh * E;
             const float4* xs = reinterpret_cast<const float4*>(xbuf) + (p * H + hh) * (E / 2) * N + j;
             float ur[E], ui[E];
@@ -338,7 +365,7 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
         gqtc::tmem_wait_st();
         gqtc::fence_before_sync();
         __syncthreads();  // stage input complete in A; coefficients and populations written
-        if (tid == 0) {
+        if (tid == 0 && !failed) {
             gqtc::fence_after_sync();
 #pragma unroll
             for (int kc = 0; kc < T::KCH; ++kc) {
@@ -357,13 +384,19 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
 #pragma unroll
         for (int q = 1; q < T::NT; ++q) cq[q] = cs[(v * P + p) * NC + (q - 1)];
         // one thread polls the mbarrier; the others wait at the barrier instead of spinning
-        const bool ok = (tid != 0) || gqtc::mbar_wait_bounded(bar, phase, kMaxPolls);
+        const bool ok = (tid != 0) || failed || gqtc::mbar_wait_bounded(bar, phase, kMaxPolls);
         const bool bad = __syncthreads_or(!ok);  // MMA complete (or given up, uniformly over the CTA)
         if constexpr (T::CL == 1) {
             if (bad) return false;
         }
+        if (bad) {
+            failed = true;
+            mma_lost = true;
+        }
         float Kr[E], Ki[E], ur[E], ui[E];
-        if (!bad) {  // (a cluster CTA whose wait gave up skips to the barrier that tells the partner)
+#pragma unroll
+        for (int e = 0; e < E; ++e) Kr[e] = Ki[e] = 0.f;
+        if (!failed) {  // (a cluster CTA that gave up sends zeros)
             phase ^= 1u;
             gqtc::fence_after_sync();
 #pragma unroll
@@ -406,25 +439,25 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
                     Ki[e] = fmaf(dv.re, ui[e], fmaf(dv.im, ur[e], Ki[e]));
                 }
             }
+        }  // !failed
+        {
             // K[n][j] for the rows n of this thread goes to the CTA that reads row j of K transposed
             // (16-byte stores: LDK even, n0 a multiple of 8)
             const int kdst = j / NH;
             const int kidx = (p * NH + (j - kdst * NH)) * LDK + n0;
-            if constexpr (T::CL > 1) {
-                const uint32_t ka = (kdst != crank ? gqtc::cluster_peer_u32(kbuf, peer) : gqtc::smem_u32(kbuf)) +
-                                    (uint32_t)kidx * 8u;
+            if (T::CL > 1 && kdst != crank) {
+                const uint32_t ka = gqtc::cluster_peer_u32(kbuf, peer) + (uint32_t)kidx * 8u;
+                const uint32_t kb = gqtc::cluster_peer_u32(kbar, peer);
 #pragma unroll
-                for (int e = 0; e < E; e += 2) gqtc::st_cluster_v4(ka + 8u * e, Kr[e], Ki[e], Kr[e + 1], Ki[e + 1]);
+                for (int e = 0; e < E; e += 2) gqtc::st_async_v4(ka + 8u * e, Kr[e], Ki[e], Kr[e + 1], Ki[e + 1], kb);
             } else {
                 float4* const kb = reinterpret_cast<float4*>(kbuf + kidx);
 #pragma unroll
                 for (int e = 0; e < E; e += 2) kb[e / 2] = make_float4(Kr[e], Ki[e], Kr[e + 1], Ki[e + 1]);
             }
-        }  // !bad
+        }
         if constexpr (T::CL > 1) {
-            if (tid == 0 && bad) *gqtc::cluster_peer(fail_flag, peer) = 1u;
-            gqtc::cluster_sync();  // K complete in both CTAs; a failure is known to both
-            if (bad || *reinterpret_cast<volatile uint32_t*>(fail_flag) != 0u) return false;
+            exchange_wait(kbar, kphase, T::KX_BYTES);  // the partner's K entries; this CTA's own ones
         } else {
             __syncthreads();  // K complete
         }
@@ -537,7 +570,6 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
     // (t_in + 0 for n = 0), s = 1, 2 at t_mid = (n + 1/2) dt, s = 3 at t_mid + dt/2 - the times and
     // roundings of gqfixed::RK4, whose coefficients come from the table (block step / KB). The next
     // block's table is filled during the MMA of stage 1 of a block's last step.
-    bool failed = false;
     {
         float kre[E], kim[E];
 #pragma unroll
@@ -550,8 +582,9 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
             const int sb = step % T::KB;
             const int ver = ((step / T::KB) & 1) * T::TS + 3 * sb + (s == 0 ? 0 : (s == 3 ? 2 : 1));
             const int fill = (s == 1 && sb == T::KB - 1) ? step / T::KB + 1 : -1;
-            if (!eval(kre, kim, it & 1, ver, fill)) {
+            if (!eval(kre, kim, it & 1, ver, fill)) {  // (a single CTA only)
                 failed = true;
+                mma_lost = true;
                 break;
             }
             const int nslot = (it + 1) & 1;
@@ -605,10 +638,15 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
         }
     }
 
+    if constexpr (T::CL > 1) {  // a failure of either CTA fails the tile (one cluster barrier, both CTAs)
+        if (tid == 0 && failed) *gqtc::cluster_peer(fail_flag, peer) = 1u;
+        gqtc::cluster_sync();
+        if (*reinterpret_cast<volatile uint32_t*>(fail_flag) != 0u) failed = true;
+    }
     float* out = static_cast<float*>(d.results);
     if (failed) {
-        // the MMA of the last phase did not signal: wait once more (bounded), mark the tile's outputs
-        gqtc::mbar_wait_bounded(bar, phase, kMaxPolls);
+        // an MMA that did not signal: wait once more for it (bounded); mark the tile's outputs
+        if (mma_lost && tid == 0) gqtc::mbar_wait_bounded(bar, phase, kMaxPolls);
         if (active && lead && crank == 0) {
             const int width = (OUT == GQIS_OUT_FINAL_STATE) ? MM::S : 2;
             for (int i = 0; i < width; ++i) out[(size_t)local * width + i] = __int_as_float(0x7fc00000);

@@ -49,6 +49,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
+// One arrival on `bar` that also expects `bytes` more transaction bytes in the current phase.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
 // Polls until the phase with `parity` completed, at most `max_polls` times; false on give-up.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint32_t max_polls) {
     for (uint32_t i = 0; i < max_polls; ++i)
@@ -133,6 +137,13 @@ __device__ __forceinline__ uint32_t cluster_peer_u32(const void* p, uint32_t ran
 }
 __device__ __forceinline__ void st_cluster_v4(uint32_t addr, float a, float b, float c, float d) {
     asm volatile("st.shared::cluster.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "f"(a), "f"(b), "f"(c), "f"(d)
+                 : "memory");
+}
+// 16-byte store into another CTA's shared memory that, once it has landed, counts its bytes on that
+// CTA's mbarrier `rbar` (both shared::cluster addresses in the same CTA)
+__device__ __forceinline__ void st_async_v4(uint32_t addr, float a, float b, float c, float d, uint32_t rbar) {
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v4.f32 [%0], {%1, %2, %3, %4}, [%5];"
+                 ::"r"(addr), "f"(a), "f"(b), "f"(c), "f"(d), "r"(rbar)
                  : "memory");
 }
 
