@@ -460,8 +460,8 @@ TENSOR_DIMS = (8, 16, 32, 64)
 SMEM_LIMIT = 232448  # shared memory of one CTA on sm_100a (bytes)
 # Padded dimension from which a tile is split over a cluster of two CTAs. Only N = 64 needs it (one
 # SM's registers cannot hold the tile); splitting N = 16 / 32 tiles as well, which would let two CTAs
-# share an SM, measured 2x slower (30 -> 67 ms, 146 -> 290 ms for 4096 points x 2000 steps): the two
-# cluster barriers and remote stores of every stage cost more than the overlap gains.
+# share an SM, measured slower (30 -> 44 ms, 146 -> 212 ms for 4096 points x 2000 steps): the exchange
+# of every stage costs more than the overlap of one CTA's MMA with the other's epilogue gains.
 TC_CLUSTER_FROM = 64
 
 
