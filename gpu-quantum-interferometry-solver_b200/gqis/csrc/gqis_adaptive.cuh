@@ -297,7 +297,7 @@ struct Lane {
 #endif
 
 template <class Pair, class M, class F, int OUT, int TRACE>
-__global__ void __launch_bounds__(GQ_BLOCK) sweep_adaptive_kernel(const gqis_sweep_desc d) {
+__global__ void __launch_bounds__(GQ_BLOCK, GQ_MIN_BLOCKS) sweep_adaptive_kernel(const gqis_sweep_desc d) {
     const unsigned lane_id = threadIdx.x & 31u;
     const double rtol = d.solver_params[0], atol = d.solver_params[1];
     const int max_substeps = (int)d.solver_params[2];
