@@ -77,3 +77,41 @@ def test_two_gloo_ranks_assemble_the_one_process_map(tmp_path):
     for r in range(2):
         np.testing.assert_array_equal(np.load(tmp_path / f"rank{r}.npy"), single)
         assert float(np.load(tmp_path / f"max{r}.npy")) == 2.0
+
+
+def _fit_maps():
+    """A synthetic 7 x 5 model map, its gradient in 3 parameters and a measured map."""
+    rng = np.random.default_rng(3)
+    return rng.random((7, 5)), rng.standard_normal((7, 5, 3)), rng.random((7, 5))
+
+
+def _fit_rank(rank, ws, port, out):
+    import sys
+    import torch.distributed as dist
+    here = os.path.dirname(os.path.abspath(__file__))
+    sys.path.insert(0, os.path.join(here, "..", "gpu-quantum-interferometry-solver_b200"))
+    from gqis.shard import fit_loss_gradient, shard_rows
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=ws)
+    try:
+        m, g, y = _fit_maps()
+        b, e = shard_rows(m.shape[0], ws, rank)
+        loss, grad = fit_loss_gradient(m[b:e], g[b:e], y[b:e])
+        np.save(os.path.join(out, f"fit{rank}.npy"), np.concatenate([[loss], grad]))
+    finally:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def test_sharded_fit_gradient_is_the_one_process_gradient(tmp_path):
+    """Two gloo ranks each own rows of the map; one all-reduce of loss + 3 gradient sums gives every
+    rank the whole grid's least-squares loss and gradient."""
+    import torch.multiprocessing as mp
+    from gqis.shard import fit_loss_gradient
+    m, g, y = _fit_maps()
+    loss, grad = fit_loss_gradient(m, g, y)  # no process group: this process's sums
+    np.testing.assert_allclose(loss, np.sum((m - y) ** 2), rtol=1e-14)
+    np.testing.assert_allclose(grad, [2 * np.sum((m - y) * g[..., k]) for k in range(3)], rtol=1e-12)
+    port = _free_port()
+    mp.start_processes(_fit_rank, args=(2, port, str(tmp_path)), nprocs=2, start_method="spawn", join=True)
+    for r in range(2):
+        np.testing.assert_allclose(np.load(tmp_path / f"fit{r}.npy"), np.concatenate([[loss], grad]), rtol=1e-12)
