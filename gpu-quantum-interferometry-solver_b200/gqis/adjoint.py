@@ -1,7 +1,8 @@
-"""Gradients of the time-averaged observable: checkpointed discrete adjoint of RK4 (FP64).
+"""Gradients of the time-averaged (or final) observable: checkpointed discrete adjoint of RK4 (FP64).
 
 ``mean_gradient(model..., params=[...])`` returns the ``mesolve_2D`` mean map (FP64, bit-identical
-to the plain sweep) and d<O>_avg/dtheta for every point, where theta are runtime constants of the
+to the plain sweep) and d<O>_avg/dtheta for every point; with ``output="final"`` the final map
+(``output_mode="final"``) and d<O>_final/dtheta. theta are runtime constants of the
 model (e.g. Gamma1, Gamma_phi, Delta) and/or the swept parameters. ``MeanMap`` wraps it as a
 ``torch.autograd.Function`` for interferogram fitting: its backward contracts the per-point
 derivatives with the incoming map gradient.
@@ -153,22 +154,27 @@ def emit_adjoint(compiled, params):
 # ----------------------------------------------------------------------------------------
 
 def module_source(H, Drive, Col_Ops, mean_operator, tlist, *, var_arrays, params, const_values=None,
-                  runtime_consts=None, warmup_time=0.0, t_in=0.0, rho0=None, rho0_values=None, **codegen):
-    """Front end of an adjoint problem without a GPU: returns (module source, SweepLaunch, meta)."""
+                  runtime_consts=None, warmup_time=0.0, t_in=0.0, rho0=None, rho0_values=None, output="mean",
+                  **codegen):
+    """Front end of an adjoint problem without a GPU: returns (module source, SweepLaunch, meta).
+    ``output``: "mean" (d<O>_avg/dtheta) or "final" (d<O>/dtheta at the last step)."""
     from . import engine, solver
+    if output not in ("mean", "final"):
+        raise ValueError("the adjoint differentiates output 'mean' or 'final'")
     const_values = dict(const_values or {})
     runtime_consts = dict(runtime_consts or {})
     keep = [p for p in params if p in const_values or p in runtime_consts]
     holder = {}
     solver.mesolve_2D(H, Drive, Col_Ops, mean_operator, tlist, var_arrays=var_arrays,
                       const_values=const_values, runtime_consts=runtime_consts,
-                      keep_symbolic_consts=keep or None, fp64=True, output_mode="mean",
+                      keep_symbolic_consts=keep or None, fp64=True, output_mode=output,
                       warmup_time=warmup_time, t_in=t_in, rho0=rho0, rho0_values=rho0_values,
                       _prepare_only=holder, **codegen)
     launch = holder["launch"]
     adj_src, meta = emit_adjoint(launch.entry["compiled"], params)
-    source = engine.module_source(launch.entry["frag"], launch.entry["spec"], "fp64", "mean", None,
-                                  extra_code=adj_src, defines={"GQ_WITH_ADJOINT": 1})
+    source = engine.module_source(launch.entry["frag"], launch.entry["spec"], "fp64", output, None,
+                                  extra_code=adj_src,
+                                  defines={"GQ_WITH_ADJOINT": 1, "GQ_ADJOINT_FINAL": int(output == "final")})
     meta["defaults"] = {**const_values, **runtime_consts}
     return source, launch, meta
 
@@ -187,7 +193,7 @@ class Problem:
 
     def __init__(self, H, Drive, Col_Ops, mean_operator, tlist, *, var_arrays, params, const_values=None,
                  runtime_consts=None, warmup_time=0.0, t_in=0.0, rho0=None, rho0_values=None,
-                 checkpoint_every=None, **codegen):
+                 checkpoint_every=None, output="mean", **codegen):
         from . import abi, engine, solver
         import torch
         const_values = dict(const_values or {})
@@ -195,7 +201,8 @@ class Problem:
         source, launch, meta = module_source(H, Drive, Col_Ops, mean_operator, tlist, var_arrays=var_arrays,
                                              params=params, const_values=const_values,
                                              runtime_consts=runtime_consts, warmup_time=warmup_time, t_in=t_in,
-                                             rho0=rho0, rho0_values=rho0_values, **codegen)
+                                             rho0=rho0, rho0_values=rho0_values, output=output, **codegen)
+        self.output = output
         self.compiled = launch.entry["compiled"]
         self.params = meta["params"]
         self.P = meta["P"]

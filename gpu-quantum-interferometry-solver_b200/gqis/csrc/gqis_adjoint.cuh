@@ -1,7 +1,8 @@
 // gqis_adjoint.cuh - discrete adjoint of the fixed-step RK4 sweep (FP64), with checkpoints.
 //
 // For every point the kernel returns J = <O>_avg (the right-endpoint time average of the
-// forward sweep, as the mean output) and dJ/dtheta for the P parameters of the emitted adjoint
+// forward sweep, as the mean output) or, with FINAL, J = <O> at the last step (as the final output),
+// and dJ/dtheta for the P parameters of the emitted adjoint
 // struct A (runtime constants and/or the sweep parameters). The gradient is the exact derivative
 // of the discrete RK4 map (reverse-mode linearisation of gqfixed::RK4 with its stage times):
 //   1. forward: RK4 from the initial state, storing the state every C steps (checkpoints);
@@ -11,7 +12,7 @@
 //        stage s = 4..1 (input u_s, time t_s):  ub = J(u_s, t_s)^T kb_s;
 //        theta_b += (dF/dtheta)(u_s, t_s)^T kb_s;  lam_n += ub;  kb_{s-1} += c_s ub
 //      (u_2 = y + h/2 k_1, u_3 = y + h/2 k_2, u_4 = y + h k_3) and lam_m += w dO/dy for the
-//      averaged states m > warmup (w = 1 / (N - warmup)).
+//      averaged states m > warmup (w = 1 / (N - warmup)); with FINAL only lam_N = dO/dy(y_N).
 // The forward and the recomputation share rk4_step, so the recomputed states are bit-identical.
 // Scratch (caller-provided, gqis_adjoint_scratch_bytes): checkpoints and one segment of states
 // per point, laid out [slot][component][point] so a warp's accesses coalesce.
@@ -76,7 +77,7 @@ struct Step {
     }
 };
 
-template <class M, class A>
+template <class M, class A, int FINAL>
 __global__ void __launch_bounds__(GQ_BLOCK) adjoint_rk4_kernel(const gqis_adjoint_desc a) {
     constexpr int S = M::S;
     constexpr int P = A::P;
@@ -95,29 +96,30 @@ __global__ void __launch_bounds__(GQ_BLOCK) adjoint_rk4_kernel(const gqis_adjoin
     const double X = pc.Xd, Yv = pc.Yd;
     const double* C = a.adjoint_consts;
     const double dt = d.dt;
-    const double w = 1.0 / (double)(N - W);
+    const double w = FINAL ? 1.0 : 1.0 / (double)(N - W);
 
     // ---- 1. forward with checkpoints
     double y[S];
     pc.init(d, local, y);
-    double obs_sum = 0.0;
+    double obs_sum = 0.0, obs_im = 0.0;
     for (int n = 0; n < N; ++n) {
         if (n % CE == 0) {
 #pragma unroll
             for (int i = 0; i < S; ++i) ck[((size_t)(n / CE) * S + i) * npts + local] = y[i];
         }
         St::rk4_step(pc, d, n, y, nullptr);
-        if (n >= W) {
+        if (FINAL ? (n == N - 1) : (n >= W)) {
             double tk[4], Dr[M::NDRV], re, im;
             St::times(d, n, tk);
             pc.drives(tk[3], Dr);
             pc.observe(y, Dr, re, im);
             obs_sum += re;
+            obs_im = im;
         }
     }
     double* res = static_cast<double*>(d.results);
-    res[2 * (size_t)local] = obs_sum * w;
-    res[2 * (size_t)local + 1] = 0.0;
+    res[2 * (size_t)local] = FINAL ? obs_sum : obs_sum * w;
+    res[2 * (size_t)local + 1] = FINAL ? obs_im : 0.0;
     double ynext[S];  // y_{n+1} while stepping back through step n
 #pragma unroll
     for (int i = 0; i < S; ++i) ynext[i] = y[i];
@@ -145,7 +147,7 @@ __global__ void __launch_bounds__(GQ_BLOCK) adjoint_rk4_kernel(const gqis_adjoin
         for (int n = n1 - 1; n >= n0; --n) {
             double tk[4];
             St::times(d, n, tk);
-            if (n >= W) {  // seed of the averaged output at y_{n+1}
+            if (FINAL ? (n == N - 1) : (n >= W)) {  // seed of the output at y_{n+1}
                 double Da[A::ND > 0 ? A::ND : 1], g[S];
                 A::drives(tk[3], X, Yv, C, Da);
                 A::dobs(ynext, Da, X, Yv, C, g);

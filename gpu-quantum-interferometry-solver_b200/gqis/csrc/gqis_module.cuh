@@ -27,6 +27,9 @@
 #ifndef GQ_MATRIX
 #define GQ_MATRIX 0
 #endif
+#ifndef GQ_ADJOINT_FINAL
+#define GQ_ADJOINT_FINAL 0  // adjoint of the final <O> instead of the time average
+#endif
 
 namespace {
 
@@ -299,7 +302,7 @@ __attribute__((visibility("default"))) int gqis_adjoint_launch(const gqis_adjoin
     if (Form::id != GQIS_FORM_FP64) return fail(GQIS_ERR_UNSUPPORTED, "the adjoint runs in the FP64 form");
     int rc = check_desc(&a->sweep);
     if (rc != GQIS_OK) return rc;
-    if (a->sweep.warmup_steps >= a->sweep.num_steps)
+    if (!GQ_ADJOINT_FINAL && a->sweep.warmup_steps >= a->sweep.num_steps)
         return fail(GQIS_ERR_INVALID, "the adjoint differentiates a mean: needs steps after warmup");
     if (a->num_params != gqmodel::Adjoint::P)
         return fail(GQIS_ERR_INVALID, "num_params %d, module has %d", a->num_params, gqmodel::Adjoint::P);
@@ -313,7 +316,7 @@ __attribute__((visibility("default"))) int gqis_adjoint_launch(const gqis_adjoin
     if (gqmodel::Adjoint::P > 0 && !a->grad) return fail(GQIS_ERR_INVALID, "grad buffer is NULL");
     if (a->sweep.point_count == 0) return GQIS_OK;
     const int64_t grid = (a->sweep.point_count + GQ_BLOCK - 1) / GQ_BLOCK;
-    gqadjoint::adjoint_rk4_kernel<Model, gqmodel::Adjoint>
+    gqadjoint::adjoint_rk4_kernel<Model, gqmodel::Adjoint, GQ_ADJOINT_FINAL>
         <<<(unsigned)grid, GQ_BLOCK, 0, static_cast<cudaStream_t>(stream)>>>(*a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "adjoint kernel launch");

@@ -149,11 +149,12 @@ int gqis_sweep_launch_noalloc(const gqis_sweep_desc* desc, void* stream);
  * constants and/or sweep parameters), by the discrete adjoint of the RK4 steps with checkpoints.
  * --------------------------------------------------------------------------------------- */
 typedef struct gqis_adjoint_desc {
-    gqis_sweep_desc sweep;          /* grid, steps, warmup, dt, t_in, inputs; results = [points, 2] FP64 */
+    gqis_sweep_desc sweep;          /* grid, steps, warmup, dt, t_in, inputs; results = [points, 2] FP64:
+                                       <O>_avg, or the final <O> in a module built for the final output */
     int32_t num_params;             /* P; must equal the module's */
     int32_t checkpoint_every;       /* steps between stored states (ceil(sqrt(num_steps)) balances memory and time) */
     const double* adjoint_consts;   /* full runtime-constant array in the adjoint's order, or NULL */
-    double* grad;                   /* [point_count, P] d<O>_avg / dtheta */
+    double* grad;                   /* [point_count, P] d<O>_avg / dtheta (or d<O>_final / dtheta) */
     double* scratch;                /* gqis_adjoint_scratch_bytes() bytes of device memory (checkpoints) */
     int64_t scratch_bytes;
 } gqis_adjoint_desc;
@@ -164,7 +165,7 @@ int gqis_adjoint_info(int32_t* num_params, int32_t* state_size);
 /* Device scratch needed by gqis_adjoint_launch for this many points, steps and checkpoint interval. */
 int gqis_adjoint_scratch_bytes(int64_t point_count, int32_t num_steps, int32_t checkpoint_every, int64_t* bytes);
 
-/* Mean map and its parameter gradient; asynchronous on stream. */
+/* Mean (or final) map and its parameter gradient; asynchronous on stream. */
 int gqis_adjoint_launch(const gqis_adjoint_desc* desc, void* stream);
 
 #ifdef __cplusplus

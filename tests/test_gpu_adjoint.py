@@ -67,3 +67,32 @@ def test_autograd_backward_contracts_the_gradient():
     expect = (weights.unsqueeze(-1) * grad).sum(dim=(0, 1)).cpu()
     assert torch.allclose(theta.grad, expect, rtol=1e-12, atol=0)
     assert torch.isfinite(theta.grad).all()
+
+
+@pytest.mark.gpu
+def test_adjoint_of_the_final_observable():
+    """output="final": the final <O> map equals the plain FP64 sweep's final output, and its gradient
+    in the fit parameters (Gamma1, Gamma_phi, Delta) and the swept drive amplitude A equals central
+    differences of that sweep (h = 1e-6)."""
+    import gqis
+    from gqis import adjoint
+    args, kwargs, params = qubit_fit_model()
+    final, grad = adjoint.mean_gradient(*args, **kwargs, params=list(params), output="final")
+    plain = gqis.mesolve_2D(*args, **kwargs, keep_symbolic_consts=list(params[:3]), fp64=True, output_mode="final")
+    assert _scaled(final, plain.real) < 1e-13
+    h = 1e-6
+    base = kwargs["runtime_consts"]
+    for m, p in enumerate(params[:3]):
+        up, dn = dict(base), dict(base)
+        up[p] = base[p] + h
+        dn[p] = base[p] - h
+        fp = gqis.mesolve_2D(*args, **dict(kwargs, runtime_consts=up), fp64=True, output_mode="final").real
+        fm = gqis.mesolve_2D(*args, **dict(kwargs, runtime_consts=dn), fp64=True, output_mode="final").real
+        assert _scaled(grad[..., m], (fp - fm) / (2 * h)) < 1e-6, p
+    eps, A = list(kwargs["var_arrays"])
+    up, dn = dict(kwargs["var_arrays"]), dict(kwargs["var_arrays"])
+    up[A] = up[A] + h
+    dn[A] = dn[A] - h
+    fp = gqis.mesolve_2D(*args, **dict(kwargs, var_arrays=up), fp64=True, output_mode="final").real
+    fm = gqis.mesolve_2D(*args, **dict(kwargs, var_arrays=dn), fp64=True, output_mode="final").real
+    assert _scaled(grad[..., 3], (fp - fm) / (2 * h)) < 1e-6

@@ -112,6 +112,10 @@ def calls():
     _, args, kwargs = duffing_case(side=16, solver="rk4")  # state trace binned by the rasteriser tests
     kwargs.pop("adaptive_options")
     out.append(("odesolve_2D", args, kwargs))
+    args, kwargs, params = qubit_fit_model()  # the final-output adjoint's plain FP64 references
+    out.append(("mesolve_2D", args, dict(kwargs, fp64=True, output_mode="final")))
+    out.append(("mesolve_2D", args, dict(kwargs, keep_symbolic_consts=list(params[:3]), fp64=True,
+                                         output_mode="final")))
     return out
 
 
@@ -131,7 +135,8 @@ def qubit_fit_model(side=(8, 6), steps=400, duration=20.0):
 def adjoint_problems():
     """(args, kwargs) of the adjoint problems the GPU tests and the serving bench build."""
     args, kwargs, params = qubit_fit_model()
-    out = [(args, dict(kwargs, params=list(params))), (args, dict(kwargs, params=list(params[:3])))]
+    out = [(args, dict(kwargs, params=list(params))), (args, dict(kwargs, params=list(params[:3]))),
+           (args, dict(kwargs, params=list(params), output="final"))]
     args, kwargs, params = qubit_fit_model(side=(256, 256), steps=4000, duration=200.0)
     out.append((args, dict(kwargs, params=list(params[:3]))))
     return out
