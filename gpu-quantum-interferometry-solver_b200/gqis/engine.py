@@ -150,10 +150,28 @@ class ModelModule:
         abi.check(rc, self.lib)
 
 
+def include_dirs_digest(flags) -> str:
+    """Hash of the header files in the ``-I`` directories of ``flags`` (a caller's own template
+    directory, ``kernel_template_file``): a module built from edited headers gets a new cache key."""
+    h = hashlib.sha256()
+    for flag in flags:
+        if not flag.startswith("-I"):
+            continue
+        root = Path(flag[2:])
+        if not root.is_dir():
+            continue
+        for path in sorted(root.iterdir()):
+            if path.is_file() and path.suffix in (".cuh", ".h", ".hpp", ".hh", ".inc", ".cu"):
+                h.update(path.name.encode() + b"\0")
+                h.update(path.read_bytes())
+    return h.hexdigest()
+
+
 def build_module(source: str, *, extra_flags=(), quiet=True) -> Path:
     """Compile ``source`` into a cached shared library; returns its path."""
     flags = tuple(extra_flags)
-    key = hashlib.sha256((source + "\0" + templates_digest(source) + "\0" + " ".join(flags)).encode()).hexdigest()[:24]
+    key = hashlib.sha256((source + "\0" + templates_digest(source) + "\0" + " ".join(flags) + "\0" +
+                          include_dirs_digest(flags)).encode()).hexdigest()[:24]
     out_dir = cache_dir()
     so_path = out_dir / f"gqis_model_{key}.so"
     if so_path.exists():
@@ -163,9 +181,12 @@ def build_module(source: str, *, extra_flags=(), quiet=True) -> Path:
         cu = Path(tmp) / f"gqis_model_{key}.cu"
         cu.write_text(source)
         tmp_so = Path(tmp) / so_path.name
+        # a caller's include directories (kernel_template_file) are searched before the packaged ones
+        includes = [f for f in flags if f.startswith("-I")]
+        others = [f for f in flags if not f.startswith("-I")]
         cmd = [nvcc, *ARCH_FLAGS, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
                "-Xcompiler", "-fvisibility=hidden", "-Xptxas", "-v", "--expt-relaxed-constexpr",
-               f"-I{CSRC_DIR}", f"-I{INCLUDE_DIR}", *flags, str(cu), "-o", str(tmp_so)]
+               *includes, f"-I{CSRC_DIR}", f"-I{INCLUDE_DIR}", *others, str(cu), "-o", str(tmp_so)]
         proc = subprocess.run(cmd, capture_output=True, text=True)
         if proc.returncode != 0:
             raise RuntimeError(f"nvcc failed for a model module ({cu.name}):\n{proc.stderr[-6000:]}")

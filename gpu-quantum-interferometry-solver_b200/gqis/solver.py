@@ -469,7 +469,7 @@ def _solve_symbolic_system(H, Drive, Col_Ops, mean_operator, tlist,
     if kernel_template_file is not None:
         if not os.path.exists(kernel_template_file):
             raise FileNotFoundError(f"CUDA kernel template was not found: {kernel_template_file}")
-        template_dir = (kernel_template_file if os.path.isdir(kernel_template_file)
+        template_dir = (os.path.abspath(kernel_template_file) if os.path.isdir(kernel_template_file)
                         else os.path.dirname(os.path.abspath(kernel_template_file)))
     form = _resolve_precision(precision, fp64)
     t_in = float(t_in)

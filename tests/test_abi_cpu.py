@@ -119,3 +119,33 @@ def test_density_matrix_modules_export_the_module_entry_points(rhs_form, precisi
         assert hasattr(lib, name), name
     src = Path(str(path).replace(".so", ".cu")).read_text()
     assert ("#define GQ_MATRIX 2" in src) == (rhs_form == "matrix_tc")
+
+
+def test_module_cache_key_follows_the_callers_template_headers(tmp_path):
+    """A module built with a caller's template directory (kernel_template_file) is rebuilt when a
+    header there changes, and found again when it is restored."""
+    from gqis import engine
+    (tmp_path / "extra.cuh").write_text("#define GQIS_TEST_VALUE 1\n")
+    src = '#include "extra.cuh"\nextern "C" int gqis_test_value(void) { return GQIS_TEST_VALUE; }\n'
+    flags = (f"-I{tmp_path}",)
+    first = engine.build_module(src, extra_flags=flags)
+    (tmp_path / "extra.cuh").write_text("#define GQIS_TEST_VALUE 2\n")
+    second = engine.build_module(src, extra_flags=flags)
+    assert first != second
+    (tmp_path / "extra.cuh").write_text("#define GQIS_TEST_VALUE 1\n")
+    assert engine.build_module(src, extra_flags=flags) == first
+
+
+def test_callers_template_directory_is_searched_before_the_packaged_headers(tmp_path):
+    """kernel_template_file names a directory searched before the packaged CUDA templates: a header
+    there with a packaged header's name replaces it in the build."""
+    import ctypes
+    from gqis import engine
+    (tmp_path / "gqis_b200.h").write_text("#define GQIS_TEMPLATE_OVERRIDE 7\n")
+    src = ('#include "gqis_b200.h"\n#ifndef GQIS_TEMPLATE_OVERRIDE\n#define GQIS_TEMPLATE_OVERRIDE 0\n#endif\n'
+           'extern "C" __attribute__((visibility("default"))) int gqis_test_override(void) '
+           '{ return GQIS_TEMPLATE_OVERRIDE; }\n')
+    lib = ctypes.CDLL(str(engine.build_module(src, extra_flags=(f"-I{tmp_path}",))))
+    assert lib.gqis_test_override() == 7
+    lib = ctypes.CDLL(str(engine.build_module(src)))
+    assert lib.gqis_test_override() == 0
