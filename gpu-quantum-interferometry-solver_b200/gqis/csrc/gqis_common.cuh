@@ -147,8 +147,9 @@ struct FormFP32 {
     __device__ __forceinline__ static float cos(float x) { return ::cosf(x); }
     __device__ __forceinline__ static float tan(float x) { return ::tanf(x); }
     __device__ __forceinline__ static void accumulate(float& y, float& c, float a, Coef<float> h) {
-        const float d = fmaf(a, h.hi, a * h.lo);  // h * a with h to ~FP64 accuracy, one rounding
-        const float v = d - c;
+        // Kahan update with h * a - c formed by two FMAs (h to ~FP64 accuracy as hi + lo). Without the
+        // compensation the four-level 2048^2 x 8000 map is 10% faster but 2.5e-6 off the FP64 form.
+        const float v = fmaf(a, h.hi, fmaf(a, h.lo, -c));
         const float s = y + v;
         c = (s - y) - v;
         y = s;
