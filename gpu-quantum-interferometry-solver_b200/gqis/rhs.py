@@ -23,6 +23,7 @@ import pickle
 import time
 from dataclasses import dataclass, field
 
+import numpy as np
 import sympy as sp
 
 from .lindblad import build_reduced_lindblad_rhs, reduced_symbols, rho_matrix_to_independent_exprs
@@ -327,13 +328,47 @@ def optimize_rhs(eqs, mean_re, mean_im, states, Drive_symbol, drive_expr, *, run
 # 2 + cache: CompiledRHS
 # ----------------------------------------------------------------------------------------
 
+def _frozen(x):
+    """Hashable, structurally compared form of a call argument (SymPy matrices become immutable)."""
+    if x is None or isinstance(x, (bool, int, float, complex, str)):
+        return x
+    if isinstance(x, sp.MatrixBase):
+        return sp.ImmutableMatrix(x)
+    if isinstance(x, dict):
+        return ("dict",) + tuple(sorted(((_frozen(k), _frozen(v)) for k, v in x.items()), key=lambda kv: str(kv[0])))
+    if isinstance(x, (list, tuple)):
+        return ("seq",) + tuple(_frozen(v) for v in x)
+    if isinstance(x, np.ndarray):
+        return ("nd", x.shape, x.dtype.str, x.tobytes())
+    return sp.sympify(x)
+
+
 def compile_rhs(H, Drive, Col_Ops, mean_operator, *, sweep_symbols, const_values=None,
                 runtime_consts=None, keep_symbolic_consts=None, auto_runtime_consts=False, rho0=None,
                 ode_size=None, pre_expand=True, collect_rho=False, factor_terms=False,
                 cse_batch_size=None, cse_simplify=False, hoist_rho_independent=True, reuse=True,
                 symbolic_workers="auto", max_symbolic_workers=None):
-    """Prepare and optimise the RHS; returns ``(CompiledRHS, "hit" | "miss")``."""
+    """Prepare and optimise the RHS; returns ``(CompiledRHS, "hit" | "miss")``.
+
+    A repeated call with the same arguments is found by a key of the arguments themselves (their
+    immutable SymPy forms) before the model is prepared and printed for the structural key; runtime
+    constant values are not part of either key (they are launch inputs).
+    """
     start = time.time()
+    raw_key = None
+    if reuse:
+        try:
+            raw_key = ("b200_rhs_args_v1", _frozen(H), _frozen(Drive), _frozen(list(Col_Ops)),
+                       _frozen(mean_operator), _frozen(tuple(sweep_symbols)), _frozen(const_values or {}),
+                       tuple(sorted(str(k) for k in (runtime_consts or {}))) if isinstance(runtime_consts, dict)
+                       else None, _frozen(keep_symbolic_consts), bool(auto_runtime_consts), _frozen(rho0),
+                       ode_size, pre_expand, collect_rho, factor_terms, cse_batch_size, cse_simplify,
+                       hoist_rho_independent)
+            hit = _RHS_CODE_CACHE.get(raw_key)
+        except (TypeError, sp.SympifyError):
+            raw_key, hit = None, None
+        if hit is not None:
+            return hit, "hit"
     model = prepare_model(H, Drive, Col_Ops, mean_operator, sweep_symbols=sweep_symbols,
                           const_values=const_values, runtime_consts=runtime_consts,
                           keep_symbolic_consts=keep_symbolic_consts,
@@ -348,11 +383,15 @@ def compile_rhs(H, Drive, Col_Ops, mean_operator, *, sweep_symbols, const_values
            None if model["rho0_exprs"] is None else tuple(sp.srepr(e) for e in model["rho0_exprs"]),
            pre_expand, collect_rho, factor_terms, cse_batch_size, cse_simplify, hoist_rho_independent)
     if reuse and key in _RHS_CODE_CACHE:
+        if raw_key is not None:
+            _RHS_CODE_CACHE[raw_key] = _RHS_CODE_CACHE[key]
         return _RHS_CODE_CACHE[key], "hit"
     if reuse:
         stored = _disk_get(key)
         if stored is not None:
             _RHS_CODE_CACHE[key] = stored
+            if raw_key is not None:
+                _RHS_CODE_CACHE[raw_key] = stored
             return stored, "hit"
 
     size = model["state_size"]
@@ -388,6 +427,8 @@ def compile_rhs(H, Drive, Col_Ops, mean_operator, *, sweep_symbols, const_values
         model=model)
     if reuse:
         _RHS_CODE_CACHE[key] = compiled
+        if raw_key is not None:
+            _RHS_CODE_CACHE[raw_key] = compiled
         _disk_put(key, compiled)
     return compiled, "miss"
 

@@ -725,6 +725,9 @@ def _solve_symbolic_system(H, Drive, Col_Ops, mean_operator, tlist,
 
     res = shape_result(results)
     tr = shape_trace(trace) if return_time_trace else None
+    # finite checks on the device, before any host copy (a reduction instead of a host pass)
+    finite_res = _all_finite(res)
+    finite_tr = _all_finite(tr) if return_time_trace else True
     if not return_device:
         res = _to_output(res, False) if not isinstance(res, np.ndarray) else res
         tr = _to_output(tr, False) if (tr is not None and not isinstance(tr, np.ndarray)) else tr
@@ -732,12 +735,12 @@ def _solve_symbolic_system(H, Drive, Col_Ops, mean_operator, tlist,
         res = res.astype(np.complex128 if form == "fp64" else np.complex64, copy=False)
         if tr is not None and trace_mode == "observable":
             tr = tr.astype(np.complex128 if form == "fp64" else np.complex64, copy=False)
-    if not _all_finite(res) and not ignore_non_finite_output:
+    if not finite_res and not ignore_non_finite_output:
         if beep_on_error:
             _beep()
         raise RuntimeError("Non-finite values detected in mesolve_2D output. Try reducing dt "
                            "(increase time samples) or check model parameters/RHS.")
-    if return_time_trace and not _all_finite(tr) and not ignore_non_finite_output:
+    if return_time_trace and not finite_tr and not ignore_non_finite_output:
         if beep_on_error:
             _beep()
         raise RuntimeError("Non-finite values detected in mesolve_2D time trace. Try reducing dt "

@@ -304,3 +304,24 @@ class TimeFunctionTests(unittest.TestCase):
         refs = {int(m) for m in re.findall(r"Const_(?:arr|d)\[(\d+)\]", code)}
         self.assertEqual(refs, set(range(len(launch.consts))))  # every index read has a value, none idle
         self.assertNotIn(5.0, launch.consts)                 # the unused constant is dropped
+
+
+def test_repeated_call_skips_model_preparation_and_follows_mutated_matrices():
+    """A repeated call is found by its arguments before the model is prepared; a matrix changed in
+    place between calls is a new model (the key holds an immutable copy of its entries)."""
+    from gqis import rhs
+    eps, A, t = sp.symbols("eps A t", real=True)
+    H = sp.Matrix([[eps / 2, 0.5], [0.5, -eps / 2]])
+    ops = [0.1 * sp.Matrix([[0, 1], [0, 0]])]
+    call = dict(sweep_symbols=(eps, A), const_values={})
+    rhs._RHS_CODE_CACHE.clear()
+    with patch.dict("os.environ", {"GQIS_DISK_CACHE": "0"}):
+        first, status = rhs.compile_rhs(H, A * sp.cos(t), ops, sp.diag(0, 1), **call)
+        assert status == "miss"
+        with patch.object(rhs, "prepare_model", side_effect=AssertionError("prepared again")):
+            again, status = rhs.compile_rhs(H, A * sp.cos(t), ops, sp.diag(0, 1), **call)
+        assert status == "hit" and again is first
+        H[0, 1] = H[1, 0] = 0.7  # the same Matrix object, new entries
+        changed, status = rhs.compile_rhs(H, A * sp.cos(t), ops, sp.diag(0, 1), **call)
+        assert status == "miss" and changed is not first
+    rhs._RHS_CODE_CACHE.clear()
