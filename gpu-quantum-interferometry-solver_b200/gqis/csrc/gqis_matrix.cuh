@@ -43,10 +43,20 @@ __device__ __forceinline__ void cmac(Cx<R>& acc, Cx<R> a, Cx<R> x) {  // acc += 
     acc.im = fma(a.re, x.im, fma(a.im, x.re, acc.im));
 }
 
-// Dynamic shared memory of the kernel: two stage-input buffers and K (rows padded by one).
+// Dynamic shared memory of the kernel: two stage-input buffers, K (rows padded by one) and, where
+// it fits one CTA's shared memory, H(t) = Heff0 + sum_k c_k(t) M_k (rows padded by one), formed once
+// per coefficient time instead of by every thread that reads an entry.
+template <class MM, class R>
+constexpr size_t smem_base_bytes() {
+    return (2 * (size_t)MM::N * MM::N + (size_t)MM::N * (MM::N + 1)) * sizeof(Cx<R>);
+}
+template <class MM, class R>
+constexpr bool h_in_smem() {
+    return smem_base_bytes<MM, R>() + (size_t)MM::N * (MM::N + 1) * sizeof(Cx<R>) <= 232448;
+}
 template <class MM, class R>
 constexpr size_t smem_bytes() {
-    return (2 * (size_t)MM::N * MM::N + (size_t)MM::N * (MM::N + 1)) * sizeof(Cx<R>);
+    return smem_base_bytes<MM, R>() + (h_in_smem<MM, R>() ? (size_t)MM::N * (MM::N + 1) * sizeof(Cx<R>) : 0);
 }
 
 template <class MM, class F, int OUT, int TRACE>
@@ -58,6 +68,8 @@ __global__ void __launch_bounds__(MM::THREADS) matrix_rk4_kernel(const gqis_swee
     extern __shared__ __align__(16) unsigned char gq_smem[];
     Cx<R>* const bufs = reinterpret_cast<Cx<R>*>(gq_smem);  // [2][NN]
     Cx<R>* const Ks = bufs + 2 * NN;                         // [N][LD]
+    constexpr bool kHs = h_in_smem<MM, R>();
+    Cx<R>* const Hs = Ks + N * LD;                           // [N][LD] H(t), if kHs
 
     const int64_t local = blockIdx.x;
     const int64_t p = d.point_begin + local;
@@ -106,10 +118,27 @@ __global__ void __launch_bounds__(MM::THREADS) matrix_rk4_kernel(const gqis_swee
 
     double c[MM::NCOEF > 0 ? MM::NCOEF : 1];
     R cr[MM::NCOEF > 0 ? MM::NCOEF : 1];
+    // H(t) entry e of the current coefficients, with the same operations wherever it is formed
+    auto h_entry = [&](int e) {
+        Cx<R> h = ldc(MM::heff(), e);
+#pragma unroll
+        for (int q = 0; q < MM::ND; ++q) {
+            const Cx<R> dq = ldc(MM::dense(q), e);
+            h.re = fma(cr[q], dq.re, h.re);
+            h.im = fma(cr[q], dq.im, h.im);
+        }
+        return h;
+    };
+    // Coefficients at time t; with kHs also H(t) into shared memory. Called between stages: the last
+    // reads of Hs (the previous stage's products) precede that stage's K barrier, and the next
+    // stage's products follow its first barrier.
     auto coef = [&](double t) {
         MM::coef(t, Xd, Yd, Cd, c);
 #pragma unroll
         for (int q = 0; q < MM::NCOEF; ++q) cr[q] = (R)c[q];
+        if constexpr (kHs) {
+            for (int e = tid; e < NN; e += MM::THREADS) Hs[(e / N) * LD + e % N] = h_entry(e);
+        }
     };
 
     // k = f(rho) for the stage input in buffer `bi` (written by every thread before the call).
@@ -128,14 +157,7 @@ __global__ void __launch_bounds__(MM::THREADS) matrix_rk4_kernel(const gqis_swee
             for (int b = 0; b < TC; ++b) col[b] = rt[m * N + c0 + b];
 #pragma unroll
             for (int a = 0; a < TR; ++a) {
-                const int hi = (r0 + a) * N + m;
-                Cx<R> h = ldc(MM::heff(), hi);
-#pragma unroll
-                for (int q = 0; q < MM::ND; ++q) {
-                    const Cx<R> dq = ldc(MM::dense(q), hi);
-                    h.re = fma(cr[q], dq.re, h.re);
-                    h.im = fma(cr[q], dq.im, h.im);
-                }
+                const Cx<R> h = kHs ? Hs[(r0 + a) * LD + m] : h_entry((r0 + a) * N + m);
 #pragma unroll
                 for (int b = 0; b < TC; ++b) cmac(kt[a][b], h, col[b]);
             }
