@@ -43,20 +43,26 @@ __device__ __forceinline__ void cmac(Cx<R>& acc, Cx<R> a, Cx<R> x) {  // acc += 
     acc.im = fma(a.re, x.im, fma(a.im, x.re, acc.im));
 }
 
-// Dynamic shared memory of the kernel: two stage-input buffers, K (rows padded by one) and, where
-// it fits one CTA's shared memory, H(t) = Heff0 + sum_k c_k(t) M_k (rows padded by one), formed once
-// per coefficient time instead of by every thread that reads an entry.
+// Dynamic shared memory of the kernel: the stage input (two buffers, or one and a barrier more per
+// stage), K (rows padded by one) and H(t) = Heff0 + sum_k c_k(t) M_k (rows padded by one), formed once
+// per coefficient time instead of by every thread that reads an entry. Layouts in order of
+// preference, the first that fits one CTA (227 KB): two buffers + H, one buffer + H, two buffers.
+constexpr size_t kSmemLimit = 232448;
 template <class MM, class R>
-constexpr size_t smem_base_bytes() {
-    return (2 * (size_t)MM::N * MM::N + (size_t)MM::N * (MM::N + 1)) * sizeof(Cx<R>);
+constexpr size_t smem_layout_bytes(int buffers, bool with_h) {
+    return ((size_t)buffers * MM::N * MM::N + (size_t)(with_h ? 2 : 1) * MM::N * (MM::N + 1)) * sizeof(Cx<R>);
 }
 template <class MM, class R>
 constexpr bool h_in_smem() {
-    return smem_base_bytes<MM, R>() + (size_t)MM::N * (MM::N + 1) * sizeof(Cx<R>) <= 232448;
+    return smem_layout_bytes<MM, R>(1, true) <= kSmemLimit;
+}
+template <class MM, class R>
+constexpr int stage_buffers() {
+    return (smem_layout_bytes<MM, R>(2, true) <= kSmemLimit || !h_in_smem<MM, R>()) ? 2 : 1;
 }
 template <class MM, class R>
 constexpr size_t smem_bytes() {
-    return smem_base_bytes<MM, R>() + (h_in_smem<MM, R>() ? (size_t)MM::N * (MM::N + 1) * sizeof(Cx<R>) : 0);
+    return smem_layout_bytes<MM, R>(stage_buffers<MM, R>(), h_in_smem<MM, R>());
 }
 
 template <class MM, class F, int OUT, int TRACE>
@@ -66,9 +72,10 @@ __global__ void __launch_bounds__(MM::THREADS) matrix_rk4_kernel(const gqis_swee
     constexpr int NO = MM::NO;
     static_assert((N / TR) * COLT == MM::THREADS && MM::THREADS % 32 == 0, "tile layout");
     extern __shared__ __align__(16) unsigned char gq_smem[];
-    Cx<R>* const bufs = reinterpret_cast<Cx<R>*>(gq_smem);  // [2][NN]
-    Cx<R>* const Ks = bufs + 2 * NN;                         // [N][LD]
     constexpr bool kHs = h_in_smem<MM, R>();
+    constexpr int NB = stage_buffers<MM, R>();
+    Cx<R>* const bufs = reinterpret_cast<Cx<R>*>(gq_smem);  // [NB][NN]
+    Cx<R>* const Ks = bufs + NB * NN;                        // [N][LD]
     Cx<R>* const Hs = Ks + N * LD;                           // [N][LD] H(t), if kHs
 
     const int64_t local = blockIdx.x;
@@ -143,7 +150,7 @@ __global__ void __launch_bounds__(MM::THREADS) matrix_rk4_kernel(const gqis_swee
 
     // k = f(rho) for the stage input in buffer `bi` (written by every thread before the call).
     auto rhs = [&](int bi) {
-        const Cx<R>* __restrict__ rt = bufs + bi * NN;
+        const Cx<R>* __restrict__ rt = bufs + (NB > 1 ? bi : 0) * NN;
         __syncthreads();  // stage input complete; previous readers of Ks are done
         Cx<R> kt[TR][TC];
 #pragma unroll
@@ -206,7 +213,8 @@ __global__ void __launch_bounds__(MM::THREADS) matrix_rk4_kernel(const gqis_swee
     };
 
     auto write_stage = [&](int bi, R s) {  // buffer bi <- y + s k
-        Cx<R>* __restrict__ w = bufs + bi * NN;
+        if constexpr (NB == 1) __syncthreads();  // the previous stage input is no longer read
+        Cx<R>* __restrict__ w = bufs + (NB > 1 ? bi : 0) * NN;
 #pragma unroll
         for (int a = 0; a < TR; ++a)
 #pragma unroll
