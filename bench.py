@@ -377,8 +377,33 @@ def run_duffing(args):
                           "chaotic_points": int(chaotic.sum())},
         "clocks": clocks, "gpu_launches": args.steps,
     }
+    if args.reference_gpu and args.solver == "tsit5a" and side == 1024:
+        line["reference_kernel_gpu"] = reference_tsit5a_gpu(torch, model, d, opts, flush)
     print(json.dumps(line))
     return 0
+
+
+def reference_tsit5a_gpu(torch, model, d, opts, flush):
+    """The reference's own generated tsit5a kernel for the Duffing sweep (1024^2, final state, no
+    trace), compiled for sm_100a, against our Tsit5A on the same call without the trace."""
+    import numpy as np
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import ref_kernels
+    from gqis import solver
+    case = "duffing_tsit5a_full_final"
+    if not ref_kernels.available(case, "gpu"):
+        return None
+    call = dict(var_arrays=d["var_arrays"], y0_values=d["y0_values"], solver="tsit5a", fp64=True,
+                adaptive_options={k: v for k, v in opts.items() if k != "count_steps"})
+    ours = solver.prepare_sweep("odesolve_2D", *model, **call)
+    ms = float(np.mean(time_launches(torch, ours, 2, 1, flush)))
+    mine = ours.results.cpu().numpy()
+    ref_kernels.run_case(case, "gpu")
+    res, dt = ref_kernels.run_case(case, "gpu", repeats=2)
+    ref = np.asarray(res["result"]).reshape(mine.shape)
+    return {"reference_ms": dt * 1e3, "ours_ms_without_trace": ms, "speedup": dt * 1e3 / ms,
+            "max_abs_diff": float(np.max(np.abs(mine - ref))),
+            "points_differing_by_more_than_1e-6": int(np.sum(np.max(np.abs(mine - ref), axis=-1) > 1e-6))}
 
 
 def run_hilbert(args):

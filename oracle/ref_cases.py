@@ -85,6 +85,13 @@ def cases():
                    "return_time_trace": True,
                    "adaptive_options": {"step_rtol": 1e-8, "step_atol": 1e-10, "max_substeps": 4000}},
         "cpu": True}
+    d_full = W.duffing(side=None)  # config C3 at full size (1024^2), final state: timing on the GPU
+    out["duffing_tsit5a_full_final"] = {
+        "api": "odesolve_2D", "args": [d_full["rhs"], d_full["states"], None, d_full["tlist"]],
+        "kwargs": {"var_arrays": d_full["var_arrays"], "y0_values": d_full["y0_values"], "solver": "tsit5a",
+                   "fp64": True,
+                   "adaptive_options": {"step_rtol": 1e-8, "step_atol": 1e-10, "max_substeps": 2000}},
+        "cpu": False}
     out["duffing_rk4_observable_trace"] = {
         "api": "odesolve_2D", "args": [d["rhs"], d["states"], None, np.linspace(0.0, 50.0, 5001)],
         "kwargs": {"var_arrays": d["var_arrays"], "y0_values": d["y0_values"], "fp64": True,
