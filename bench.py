@@ -406,6 +406,54 @@ def reference_tsit5a_gpu(torch, model, d, opts, flush):
             "points_differing_by_more_than_1e-6": int(np.sum(np.max(np.abs(mine - ref), axis=-1) > 1e-6))}
 
 
+def run_two_level(args):
+    """The two-level model at the size of the reference's published two-level benchmark (RK4, 2048^2
+    points, 10,240 steps): our FP32 form and plain FP64 form, and the reference's own generated FP32 and
+    FP64 kernels for the same call compiled for sm_100a (``oracle/_ref``), on the same GPU."""
+    import numpy as np
+    import torch
+    torch.cuda.set_device(0)
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import ref_kernels
+    from gqis import solver, workloads
+    w = workloads.two_level(full=2048, steps=10240, duration=512.0)
+    model = (w["H"], w["Drive"], w["Col_Ops"], w["mean_operator"], w["tlist"])
+    call = dict(var_arrays=w["var_arrays"], const_values=w["const_values"])
+    flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    units = 2048 * 2048 * 10240
+    sampler = ClockSampler(0).start()
+    rows, maps = {}, {}
+    for form in ("fp64", "fp32"):
+        sw = solver.prepare_sweep("mesolve_2D", *model, **call, precision=form)
+        ms = float(np.mean(time_launches(torch, sw, args.steps, args.warmup, flush)))
+        maps[f"ours_{form}"] = sw.results.double().cpu().numpy()[:, 0].reshape(2048, 2048)
+        rows[f"ours_{form}"] = {"ms": ms, "points_steps_per_s": units / (ms / 1e3)}
+        del sw
+    for form in ("fp64", "fp32"):
+        case = f"c1_big_{form}_mean"
+        if not ref_kernels.available(case, "gpu"):
+            continue
+        ref_kernels.run_case(case, "gpu")
+        res, dt = ref_kernels.run_case(case, "gpu", repeats=args.steps)
+        maps[f"reference_{form}"] = np.asarray(res["result"]).real.reshape(2048, 2048)
+        rows[f"reference_{form}"] = {"ms": dt * 1e3, "points_steps_per_s": units / dt}
+    clocks = sampler.stop()
+    for key in rows:
+        rows[key]["max_abs_vs_our_fp64"] = float(np.max(np.abs(maps[key] - maps["ours_fp64"])))
+    line = {
+        "metric": "points*steps/s (RK4, two-level Lindblad sweep at the reference's published benchmark size)",
+        "value": rows["ours_fp32"]["points_steps_per_s"], "unit": "points*steps/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": rows["ours_fp32"]["ms"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "two-level driven qubit (H = eps/2 sz + 1/2 sx + A cos(pi t) sz, sqrt(0.01) s-, "
+                               "sqrt(0.01) sz), 2048 x 2048 (eps, A), 10,240 RK4 steps of dt 0.05, mean <|1><1|>",
+                   "l2": "flushed (256 MiB write) between timed launches"},
+        "forms": rows, "reference_published_rtx3080_fp32": 1.19e11, "clocks": clocks,
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def run_hilbert(args):
     """Config C4: Hilbert-space scaling of the density-matrix kernel, N in {8, 16, 32, 64}, 64 x 64
     (eps, A) points, 2000 RK4 steps on [0, 100]; FP64 and FP32 forms, error vs the FP64 oracle."""
@@ -761,7 +809,7 @@ def main():
     ap.add_argument("--forms", default="", help="hilbert: comma list of forms to run (e.g. matrix_tc_fp32); all if empty")
     ap.add_argument("--hsteps", type=int, default=2000, help="hilbert: RK4 steps (t spans 100 * hsteps / 2000)")
     ap.add_argument("--workload", default="four_level",
-                    choices=("four_level", "duffing", "serving", "hilbert", "render", "fit"),
+                    choices=("four_level", "two_level", "duffing", "serving", "hilbert", "render", "fit"),
                     help="four_level: the headline RK4 interferogram; duffing: the adaptive ODE sweep")
     ap.add_argument("--solver", default="dop853a", help="adaptive solver of --workload duffing")
     args = ap.parse_args()
@@ -771,6 +819,8 @@ def main():
         return run_duffing(args)
     if args.workload == "serving":
         return run_serving(args)
+    if args.workload == "two_level":
+        return run_two_level(args)
     if args.workload == "hilbert":
         return run_hilbert(args)
     if args.workload == "render":

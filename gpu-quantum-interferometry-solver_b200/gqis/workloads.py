@@ -36,7 +36,7 @@ def _axis(lo, hi, full, side):
     return values[idx]
 
 
-def two_level(side=None):
+def two_level(side=None, full=64, steps=4000, duration=200.0):
     eps, A, Delta, Drive, t = sp.symbols("eps A Delta Drive t", real=True)
     sz = sp.Matrix([[1, 0], [0, -1]])
     sx = sp.Matrix([[0, 1], [1, 0]])
@@ -45,8 +45,8 @@ def two_level(side=None):
     drive = A * sp.cos(2 * sp.pi * 0.5 * t)
     col = [sp.sqrt(0.01) * sm, sp.sqrt(0.02 / 2) * sz]
     return {"name": "two_level", "H": H, "Drive": drive, "Col_Ops": col, "mean_operator": sp.diag(0, 1),
-            "tlist": np.linspace(0.0, 200.0, 4001),
-            "var_arrays": {eps: _axis(-5.0, 5.0, 64, side), A: _axis(0.0, 5.0, 64, side)},
+            "tlist": np.linspace(0.0, duration, steps + 1),
+            "var_arrays": {eps: _axis(-5.0, 5.0, full, side), A: _axis(0.0, 5.0, full, side)},
             "const_values": {Delta: 1.0}, "symbols": (eps, A), "N": 2,
             "omega": 2 * np.pi * 0.5}
 

@@ -85,6 +85,11 @@ def cases():
                    "return_time_trace": True,
                    "adaptive_options": {"step_rtol": 1e-8, "step_atol": 1e-10, "max_substeps": 4000}},
         "cpu": True}
+    # the two-level model at the size of the reference's published two-level benchmark (2048^2 points,
+    # 10,240 RK4 steps): timing on the GPU
+    big = W.two_level(full=2048, steps=10240, duration=512.0)
+    out["c1_big_fp64_mean"] = dict(_lindblad(big, fp64=True), cpu=False)
+    out["c1_big_fp32_mean"] = dict(_lindblad(big, fp64=False), cpu=False)
     d_full = W.duffing(side=None)  # config C3 at full size (1024^2), final state: timing on the GPU
     out["duffing_tsit5a_full_final"] = {
         "api": "odesolve_2D", "args": [d_full["rhs"], d_full["states"], None, d_full["tlist"]],
