@@ -61,10 +61,10 @@ struct TcShape {
     static constexpr int CL = MM::TC_CL;      // CTAs per tile (cluster size, chosen by the model emitter)
     static constexpr int NH = N / CL;         // rows n of every column held by one CTA
     static constexpr int P = 128 / N;         // points per tile
-    static constexpr int E = 8;               // rows of a column per thread
+    static constexpr int E = MM::TC_E;        // rows of a column per thread (4 or 8, chosen by the emitter)
     static constexpr int H = NH / E;          // threads per column in one CTA
     static constexpr int THREADS = 128 * H;
-    static constexpr int MIN_CTAS = 65536 / (THREADS * 128);  // keeps <= 128 registers per thread
+    static constexpr int MIN_CTAS = 65536 / (THREADS * (E == 8 ? 128 : 64));  // registers per thread: 128 / 64
     static constexpr int NGM = MM::kDiagInMma ? MM::NG : 0;  // diagonal terms done by the MMA
     static constexpr int NT = 1 + MM::ND + NGM;      // operator terms in B
     static constexpr int NMMA = 2 * NH * NT;  // B / D columns
@@ -102,7 +102,7 @@ struct TcShape {
     static constexpr size_t SMEM = ((NEEDED > FLOOR ? NEEDED : FLOOR) + 1023) / 1024 * 1024;
     static_assert(N == 8 || N == 16 || N == 32 || N == 64, "tensor-core form: padded dimension 8, 16, 32 or 64");
     static_assert(CL == 1 || CL == 2, "one or two CTAs per tile");
-    static_assert(H >= 1 && NH % E == 0, "rows per thread");
+    static_assert((E == 4 || E == 8) && H >= 1 && NH % E == 0, "rows per thread");
     static_assert(NMMA % 16 == 0 && NMMA <= 256, "MMA N dimension");
     static_assert(COLS_USED <= 512, "tensor memory columns");
     static_assert(SMEM <= 232448, "shared memory per CTA");
@@ -298,10 +298,10 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
             pr = ur;
             pi = ui;
         }
-        gqtc::tmem_st8(t_ahi + n0, hr);
-        gqtc::tmem_st8(t_ahi + N + n0, hi_);
-        gqtc::tmem_st8(t_alo + n0, lr);
-        gqtc::tmem_st8(t_alo + N + n0, li);
+        gqtc::tmem_st<E>(t_ahi + n0, hr);
+        gqtc::tmem_st<E>(t_ahi + N + n0, hi_);
+        gqtc::tmem_st<E>(t_alo + n0, lr);
+        gqtc::tmem_st<E>(t_alo + N + n0, li);
     };
 
     uint32_t phase = 0, xphase = 0, kphase = 0;
@@ -348,8 +348,8 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
                     hv[e] = tf32_round(ur[e]);
                     lv[e] = ur[e] - hv[e];
                 }
-                gqtc::tmem_st8(t_ahi + mb, hv);
-                gqtc::tmem_st8(t_alo + mb, lv);
+                gqtc::tmem_st<E>(t_ahi + mb, hv);
+                gqtc::tmem_st<E>(t_alo + mb, lv);
             }
             {
                 float hv[E], lv[E];
@@ -358,8 +358,8 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
                     hv[e] = tf32_round(ui[e]);
                     lv[e] = ui[e] - hv[e];
                 }
-                gqtc::tmem_st8(t_ahi + N + mb, hv);
-                gqtc::tmem_st8(t_alo + N + mb, lv);
+                gqtc::tmem_st<E>(t_ahi + N + mb, hv);
+                gqtc::tmem_st<E>(t_alo + N + mb, lv);
             }
         }
         gqtc::tmem_wait_st();
@@ -401,9 +401,9 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
             gqtc::fence_after_sync();
 #pragma unroll
             for (int q = 0; q < T::NT; ++q) {
-                float a[8], b[8];
-                gqtc::tmem_ld8(t_d + (2 * q) * NH + (n0 - nb), a);
-                gqtc::tmem_ld8(t_d + (2 * q + 1) * NH + (n0 - nb), b);
+                float a[E], b[E];
+                gqtc::tmem_ld<E>(t_d + (2 * q) * NH + (n0 - nb), a);
+                gqtc::tmem_ld<E>(t_d + (2 * q + 1) * NH + (n0 - nb), b);
                 gqtc::tmem_wait_ld();
 #pragma unroll
                 for (int e = 0; e < E; ++e) {
@@ -412,11 +412,11 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
                 }
             }
             if constexpr (MM::kOwnTerms || (T::NGM < MM::NG)) {  // terms that need the stage input itself
-                float a[8], b[8], c2[8], d2[8];
-                gqtc::tmem_ld8(t_ahi + n0, a);
-                gqtc::tmem_ld8(t_ahi + N + n0, b);
-                gqtc::tmem_ld8(t_alo + n0, c2);
-                gqtc::tmem_ld8(t_alo + N + n0, d2);
+                float a[E], b[E], c2[E], d2[E];
+                gqtc::tmem_ld<E>(t_ahi + n0, a);
+                gqtc::tmem_ld<E>(t_ahi + N + n0, b);
+                gqtc::tmem_ld<E>(t_alo + n0, c2);
+                gqtc::tmem_ld<E>(t_alo + N + n0, d2);
                 gqtc::tmem_wait_ld();
 #pragma unroll
                 for (int e = 0; e < E; ++e) {

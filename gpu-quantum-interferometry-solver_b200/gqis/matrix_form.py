@@ -345,10 +345,21 @@ def diag_in_mma(mm: MatrixModel):
     return mm.Np <= 16
 
 
+# Rows of a column per thread of the tensor-core kernel, by padded dimension (4 or 8). Four rows double
+# a CTA's threads and halve each thread's epilogue chain, but measured slower (4096 points x 2000 steps:
+# N = 8 10.4 -> 11.0 ms, N = 16 30.1 -> 38.3 ms with 64 registers per thread), so every dimension uses 8.
+TC_ROWS_PER_THREAD = {8: 8, 16: 8, 32: 8, 64: 8}
+
+
+def tensor_core_rows(mm: MatrixModel):
+    return TC_ROWS_PER_THREAD.get(mm.Np, 8)
+
+
 def _tensor_core_tables(mm: MatrixModel):
-    lists, own = tensor_core_jump_lists(mm)
+    E = tensor_core_rows(mm)
+    lists, own = tensor_core_jump_lists(mm, rows_per_thread=E)
     Np = mm.Np
-    H = Np // 8
+    H = Np // E
     jmax = max(1, max(len(lists[j][b]) for j in range(Np) for b in range(H)))
     count, e, a, coef, rate = [], [], [], [], []
     for j in range(Np):
@@ -367,12 +378,13 @@ def _tensor_core_tables(mm: MatrixModel):
         _array("mm_tcj_rate", "int", rate),
         _array("mm_tcj_coef", "mreal", _interleave(coef)),
     ]
-    on_diag = all(e + 8 * b == j for j in range(Np) for b in range(H) for (e, _, _, _) in lists[j][b])
+    on_diag = all(e + E * b == j for j in range(Np) for b in range(H) for (e, _, _, _) in lists[j][b])
     members = f"""    static constexpr int TCJ_MAX = {jmax};
     static constexpr bool kOwnTerms = {'true' if own else 'false'};
     static constexpr bool kJumpsOnDiagonal = {'true' if on_diag else 'false'};
     static constexpr bool kDiagInMma = {'true' if diag_in_mma(mm) else 'false'};
     static constexpr int TC_CL = {tensor_core_shape(mm)[0]};
+    static constexpr int TC_E = {E};
     __device__ __forceinline__ static const int* tcj_count() {{ return mm_tcj_count; }}
     __device__ __forceinline__ static const int* tcj_e() {{ return mm_tcj_e; }}
     __device__ __forceinline__ static const int* tcj_a() {{ return mm_tcj_a; }}
@@ -471,7 +483,7 @@ def tensor_core_shape(mm: MatrixModel):
     Np = mm.Np
     cl = 2 if Np >= TC_CLUSTER_FROM else 1
     nh = Np // cl
-    P, E = 128 // Np, 8
+    P, E = 128 // Np, tensor_core_rows(mm)
     H = nh // E
     terms = 1 + mm.num_dense + (mm.num_diag if diag_in_mma(mm) else 0)
     nmma = 2 * nh * terms
@@ -506,9 +518,9 @@ def tensor_core_blockers(mm: MatrixModel, form: str):
     if any(src != dst and src // mm.Np != src % mm.Np for dst, src, _, _ in mm.jumps):
         out.append("a jump term moves a coherence to another element (only populations may feed other elements)")
     elif mm.Np in TENSOR_DIMS:
-        lists, _ = tensor_core_jump_lists(mm)
+        lists, _ = tensor_core_jump_lists(mm, rows_per_thread=tensor_core_rows(mm))
         if max(len(x) for col in lists for x in col) > 32:
-            out.append("more than 32 jump terms land in one thread's eight rows")
+            out.append("more than 32 jump terms land in one thread's rows")
     return out
 
 
