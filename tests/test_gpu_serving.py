@@ -86,3 +86,27 @@ def test_tensor_core_request_is_the_same_in_chunks_that_split_tiles(N):
     with SweepServer(streams=3, chunk_points=13, max_inflight=4) as srv:
         out = srv.submit("mesolve_2D", *args, **kwargs, precision="fp32", rhs_form="matrix_tc").result(300)
     np.testing.assert_array_equal(out["result"], alone)
+
+
+@pytest.mark.gpu
+def test_tensor_core_requests_of_every_tile_shape_share_the_device():
+    """Tensor-core requests of N = 8, 16 and 64 (one CTA per tile, and a two-CTA cluster per tile that
+    allocates all of its SMs' tensor memory) and a reduced-form request run concurrently on four
+    streams; each result equals the request run alone."""
+    import gqis
+    from gqis.serving import SweepServer
+    from test_support_calls import hilbert_model
+    reqs = {}
+    for N, side in ((64, (5, 3)), (16, (12, 9)), (8, (4, 3))):
+        _, args, kwargs = hilbert_model(N, side=side)
+        reqs[f"tc{N}"] = (args, dict(kwargs, precision="fp32", rhs_form="matrix_tc"))
+    case = ref_cases.cases()["c2_fp64_mean_sub32"]
+    reqs["reduced"] = (tuple(case["args"]), dict(case["kwargs"]))
+    alone = {k: gqis.mesolve_2D(*a, **kw) for k, (a, kw) in reqs.items()}
+    with SweepServer(streams=4, chunk_points=7, max_inflight=8) as srv:
+        futs = {k: srv.submit("mesolve_2D", *a, **kw) for k, (a, kw) in reqs.items()}
+        outs = {k: f.result(300) for k, f in futs.items()}
+        stats = dict(srv.stats)
+    assert stats["completed"] == len(reqs) and stats["max_concurrent"] >= 2
+    for k in reqs:
+        np.testing.assert_array_equal(outs[k]["result"], alone[k], err_msg=k)
