@@ -27,7 +27,8 @@
 // (hi*hi + hi*lo + lo*hi) with FP32 accumulation; the state is FP32 with the FP32 form's
 // compensated update, time and coefficients FP64, the mean of <O> FP64.
 //
-// Thread t: lane r = t % 128 (warp quadrant r / 32), rows n0 = nb + 8 (t / 128) .. n0 + 7 of column j.
+// Thread t: lane r = t % 128 (warp quadrant r / 32), rows n0 = nb + E (t / 128) .. n0 + E - 1 of column j
+// (E = 8 rows per thread; the emitter may choose 4).
 // Diagonal operator terms go through the MMA (kDiagInMma, small N) or the epilogue (larger N,
 // where the MMA is the longer part of a stage). Coefficients are evaluated in FP64 for every point
 // and stage time of KB steps at once, spread over all threads while an MMA runs, into a
@@ -208,7 +209,7 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
     const uint32_t idesc = gqtc::idesc_tf32_m128(T::NMMA);
     const uint32_t b_hi_addr = gqtc::smem_u32(bhi), b_lo_addr = gqtc::smem_u32(blo);
 
-    // ---- state: rows n0..n0+7 of column j, FP32 with compensation
+    // ---- state: rows n0 .. n0 + E - 1 of column j, FP32 with compensation
     float yre[E], yim[E], cre[E], cim[E], are[E], aim[E];
     {
         double pop_last = 1.0;
