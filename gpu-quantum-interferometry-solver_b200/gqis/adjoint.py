@@ -98,8 +98,27 @@ def emit_adjoint(compiled, params):
                 term += sp.diff(eqs[j], dk) * dD[k][m]
             total += kb[j] * term
         fp.append((f"tb[{m}] +=", total))
-    dr = [(f"D[{k}] =", e) for k, (_, e) in enumerate(drives)]
-    ddr = [(f"dD[{k * P + m}] =", sp.diff(e, th)) for k, (_, e) in enumerate(drives) for m, th in enumerate(theta)]
+    # Functions of time alone (cos(w t), with runtime constants at most) in the drives and their
+    # parameter derivatives are the same for every point: Tf[k], which the kernel evaluates once per
+    # warp for the stage times of a block of steps (time_funcs).
+    uniform = {str(s) for s in compiled.runtime_const_syms} | {"t"}
+    time_funcs = {}
+
+    def factor_time(e):
+        found = {}
+        walk = sp.preorder_traversal(sp.sympify(e))
+        for sub in walk:
+            names_in = {str(x) for x in sub.free_symbols} if isinstance(sub, sp.Function) else set()
+            if names_in and names_in <= uniform and "t" in names_in:
+                k = time_funcs.setdefault(sub, len(time_funcs))
+                found[sub] = sp.Symbol(f"Tf[{k}]", real=True)
+                walk.skip()
+        return sp.sympify(e).xreplace(found) if found else e
+
+    dr = [(f"D[{k}] =", factor_time(e)) for k, (_, e) in enumerate(drives)]
+    ddr = [(f"dD[{k * P + m}] =", factor_time(sp.diff(e, th)))
+           for k, (_, e) in enumerate(drives) for m, th in enumerate(theta)]
+    tf = [(f"Tf[{k}] =", f) for k, f in enumerate(sorted(time_funcs, key=time_funcs.get))]
     dob = [(f"g[{i}] =", sp.diff(mean_re, yi)) for i, yi in enumerate(states)]
 
     names = {str(d): f"D[{k}]" for k, d in enumerate(dsyms)}
@@ -120,12 +139,19 @@ def emit_adjoint(compiled, params):
     src = f"""struct Adjoint {{
     static constexpr int P = {P};
     static constexpr int ND = {ND};
-    __device__ __forceinline__ static void drives(double t, double ParX, double ParY, const double* C, double* D) {{
-        (void)t; (void)ParX; (void)ParY; (void)C; (void)D;
+    static constexpr int NTF = {len(time_funcs)};
+    __device__ __forceinline__ static void time_funcs(double t, const double* C, double* Tf) {{
+        (void)t; (void)C; (void)Tf;
+{body(fix(_lines(tf, "at")))}
+    }}
+    __device__ __forceinline__ static void drives(double t, const double* Tf, double ParX, double ParY,
+                                                  const double* C, double* D) {{
+        (void)t; (void)Tf; (void)ParX; (void)ParY; (void)C; (void)D;
 {body(fix(_lines(dr, "ad")))}
     }}
-    __device__ __forceinline__ static void ddrives(double t, double ParX, double ParY, const double* C, double* dD) {{
-        (void)t; (void)ParX; (void)ParY; (void)C; (void)dD;
+    __device__ __forceinline__ static void ddrives(double t, const double* Tf, double ParX, double ParY,
+                                                   const double* C, double* dD) {{
+        (void)t; (void)Tf; (void)ParX; (void)ParY; (void)C; (void)dD;
 {body(fix(_lines(ddr, "add")))}
     }}
     __device__ __forceinline__ static void jt(const double* u, const double* kb, const double* D, double ParX,

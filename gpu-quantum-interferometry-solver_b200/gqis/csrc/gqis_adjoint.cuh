@@ -14,6 +14,9 @@
 //      (u_2 = y + h/2 k_1, u_3 = y + h/2 k_2, u_4 = y + h k_3) and lam_m += w dO/dy for the
 //      averaged states m > warmup (w = 1 / (N - warmup)); with FINAL only lam_N = dO/dy(y_N).
 // The forward and the recomputation share rk4_step, so the recomputed states are bit-identical.
+// Functions of time alone (the model's and the adjoint struct's time_funcs, e.g. cos(w t)) come from a
+// per-warp table of the stage times of kAdjChunk steps, filled by the warp's lanes together, as in
+// gqfixed::RK4; the passes refill it as they move forward or backward through the steps.
 // Scratch (caller-provided, gqis_adjoint_scratch_bytes): checkpoints and one segment of states
 // per point, laid out [slot][component][point] so a warp's accesses coalesce.
 #pragma once
@@ -37,13 +40,24 @@ struct Step {
         tk[3] = d.t_in + (t_mid + h2);
     }
 
-    // One RK4 step with the forward kernel's rounding; optionally returns the stage inputs.
+    // Drives at time t: from the functions of time Tf (the table) where the model has any.
+    __device__ __forceinline__ static void drives(const PC& pc, double t, const double* Tf, double* Dr) {
+        if constexpr (M::NTF > 0) {
+            pc.drives_tf(t, Tf, Dr);
+        } else {
+            pc.drives(t, Dr);
+        }
+    }
+
+    // One RK4 step with the forward kernel's rounding; optionally returns the stage inputs. tf0, tf1,
+    // tf3: the model's functions of time at the step's start, midpoint and end.
     __device__ __forceinline__ static void rk4_step(const PC& pc, const gqis_sweep_desc& d, int n, double* y,
-                                                    double (*u)[S]) {
+                                                    double (*u)[S], const double* tf0, const double* tf1,
+                                                    const double* tf3) {
         const double dt = d.dt, h2 = dt * 0.5, h6 = dt / 6.0;
         double tk[4], k[S], yt[S], acc[S], Dr[M::NDRV];
         times(d, n, tk);
-        pc.drives(tk[0], Dr);
+        drives(pc, tk[0], tf0, Dr);
         pc.rhs(y, Dr, k);
 #pragma unroll
         for (int i = 0; i < S; ++i) {
@@ -52,7 +66,7 @@ struct Step {
             acc[i] = k[i];
             if (u) u[1][i] = yt[i];
         }
-        pc.drives(tk[1], Dr);
+        drives(pc, tk[1], tf1, Dr);
         pc.rhs(yt, Dr, k);
 #pragma unroll
         for (int i = 0; i < S; ++i) {
@@ -61,7 +75,7 @@ struct Step {
             if (u) u[2][i] = yt[i];
         }
         pc.rhs(yt, Dr, k);
-        pc.drives(tk[3], Dr);
+        drives(pc, tk[3], tf3, Dr);
 #pragma unroll
         for (int i = 0; i < S; ++i) {
             yt[i] = fma(dt, k[i], y[i]);
@@ -76,6 +90,25 @@ struct Step {
         }
     }
 };
+
+constexpr int kAdjChunk = 16;  // steps per table fill
+
+// Table entries e = 3 i + kind (step nb + i; kind 0: start, 1: midpoint, 2: end) of the functions of
+// time, the model's (M::NTF) then the adjoint's (A::NTF), computed by the warp's active lanes. Not
+// inlined: its FP64 transcendental code stays out of the integration loops' registers.
+template <class M, class A>
+__device__ __noinline__ void fill_adjoint_table(const gqis_sweep_desc& d, int nb, int rank, int nlanes,
+                                                const double* Cd, const double* Ca, double* tab) {
+    constexpr int W = M::NTF + A::NTF;
+    for (int e = rank; e < 3 * kAdjChunk; e += nlanes) {
+        double tk[4];
+        Step<M>::times(d, nb + e / 3, tk);
+        const int kind = e % 3;
+        const double t = kind == 0 ? tk[0] : (kind == 1 ? tk[1] : tk[3]);
+        if constexpr (M::NTF > 0) M::time_funcs(t, Cd, tab + e * W);
+        if constexpr (A::NTF > 0) A::time_funcs(t, Ca, tab + e * W + M::NTF);
+    }
+}
 
 template <class M, class A, int FINAL>
 __global__ void __launch_bounds__(GQ_BLOCK) adjoint_rk4_kernel(const gqis_adjoint_desc a) {
@@ -98,6 +131,31 @@ __global__ void __launch_bounds__(GQ_BLOCK) adjoint_rk4_kernel(const gqis_adjoin
     const double dt = d.dt;
     const double w = FINAL ? 1.0 : 1.0 / (double)(N - W);
 
+    // per-warp table of the functions of time (lanes of this warp past the grid's end have exited)
+    constexpr int TW = M::NTF + A::NTF;
+    __shared__ double tf_tab[TW > 0 ? GQ_BLOCK / 32 : 1][TW > 0 ? 3 * kAdjChunk * TW : 1];
+    double* const tab = tf_tab[TW > 0 ? (threadIdx.x >> 5) : 0];
+    const int lane = threadIdx.x & 31;
+    const int64_t valid = npts - (local - lane);
+    const unsigned warp_mask = valid >= 32 ? 0xffffffffu : ((1u << valid) - 1u);
+    const int rank = __popc(warp_mask & ((1u << lane) - 1u)), nlanes = __popc(warp_mask);
+    int cb = -(1 << 30);  // first step of the table's block
+    // entry of step n, kind 0 / 1 / 2 (start / midpoint / end); `up`: the pass moves forward in n
+    auto tf_at = [&](int n, int kind, bool up) -> const double* {
+        if constexpr (TW > 0) {
+            if (n < cb || n >= cb + kAdjChunk) {
+                const int nb = up ? n : (n >= kAdjChunk - 1 ? n - (kAdjChunk - 1) : 0);
+                __syncwarp(warp_mask);  // the previous block is consumed
+                fill_adjoint_table<M, A>(d, nb, rank, nlanes, pc.Cd, C, tab);
+                __syncwarp(warp_mask);
+                cb = nb;
+            }
+            return tab + (3 * (n - cb) + kind) * TW;
+        } else {
+            return nullptr;
+        }
+    };
+
     // ---- 1. forward with checkpoints
     double y[S];
     pc.init(d, local, y);
@@ -107,11 +165,11 @@ __global__ void __launch_bounds__(GQ_BLOCK) adjoint_rk4_kernel(const gqis_adjoin
 #pragma unroll
             for (int i = 0; i < S; ++i) ck[((size_t)(n / CE) * S + i) * npts + local] = y[i];
         }
-        St::rk4_step(pc, d, n, y, nullptr);
+        St::rk4_step(pc, d, n, y, nullptr, tf_at(n, 0, true), tf_at(n, 1, true), tf_at(n, 2, true));
         if (FINAL ? (n == N - 1) : (n >= W)) {
             double tk[4], Dr[M::NDRV], re, im;
             St::times(d, n, tk);
-            pc.drives(tk[3], Dr);
+            St::drives(pc, tk[3], tf_at(n, 2, true), Dr);
             pc.observe(y, Dr, re, im);
             obs_sum += re;
             obs_im = im;
@@ -142,14 +200,16 @@ __global__ void __launch_bounds__(GQ_BLOCK) adjoint_rk4_kernel(const gqis_adjoin
         for (int n = n0; n < n1; ++n) {
 #pragma unroll
             for (int i = 0; i < S; ++i) seg[((size_t)(n - n0) * S + i) * npts + local] = y[i];
-            if (n + 1 < n1) St::rk4_step(pc, d, n, y, nullptr);
+            if (n + 1 < n1) St::rk4_step(pc, d, n, y, nullptr, tf_at(n, 0, true), tf_at(n, 1, true), tf_at(n, 2, true));
         }
         for (int n = n1 - 1; n >= n0; --n) {
             double tk[4];
             St::times(d, n, tk);
+            const double* tfe = tf_at(n, 2, false);  // this step's end: the model's, then the adjoint's
+            const double* tfa[4] = {tf_at(n, 0, false), tf_at(n, 1, false), tf_at(n, 1, false), tfe};
             if (FINAL ? (n == N - 1) : (n >= W)) {  // seed of the output at y_{n+1}
                 double Da[A::ND > 0 ? A::ND : 1], g[S];
-                A::drives(tk[3], X, Yv, C, Da);
+                A::drives(tk[3], TW > 0 ? tfe + M::NTF : nullptr, X, Yv, C, Da);
                 A::dobs(ynext, Da, X, Yv, C, g);
 #pragma unroll
                 for (int i = 0; i < S; ++i) lam[i] = fma(w, g[i], lam[i]);
@@ -159,7 +219,7 @@ __global__ void __launch_bounds__(GQ_BLOCK) adjoint_rk4_kernel(const gqis_adjoin
             double u[4][S];
 #pragma unroll
             for (int i = 0; i < S; ++i) ynext[i] = y[i];  // y_n is y_{n+1} of the next iteration
-            St::rk4_step(pc, d, n, y, u);
+            St::rk4_step(pc, d, n, y, u, tfa[0], tfa[1], tfe);
             const double h2 = dt * 0.5, h6 = dt / 6.0;
             const double cw[4] = {h6, 2.0 * h6, 2.0 * h6, h6};
             const double cs[4] = {0.0, h2, h2, dt};
@@ -171,8 +231,9 @@ __global__ void __launch_bounds__(GQ_BLOCK) adjoint_rk4_kernel(const gqis_adjoin
 #pragma unroll
             for (int s = 3; s >= 0; --s) {
                 double Da[A::ND > 0 ? A::ND : 1], dDa[A::ND * P > 0 ? A::ND * P : 1], ub[S];
-                A::drives(tk[s], X, Yv, C, Da);
-                A::ddrives(tk[s], X, Yv, C, dDa);
+                const double* tfs = TW > 0 ? tfa[s] + M::NTF : nullptr;
+                A::drives(tk[s], tfs, X, Yv, C, Da);
+                A::ddrives(tk[s], tfs, X, Yv, C, dDa);
                 A::jt(u[s], kbs[s], Da, X, Yv, C, ub);
                 A::fparam(u[s], kbs[s], Da, dDa, X, Yv, C, tb);
 #pragma unroll
