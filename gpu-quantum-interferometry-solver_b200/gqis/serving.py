@@ -12,7 +12,7 @@ Each point's result depends only on its own inputs, so a request returns the sam
 in the mix (the GPU tests check that bit for bit).
 
 The device layer is a small backend object so that the scheduling logic (admission by memory
-budget and slots, round-robin dispatch, cancellation, failure isolation) is tested on the CPU with
+budget and slots, priority dispatch, cancellation, failure isolation) is tested on the CPU with
 a fake backend.
 """
 
@@ -95,6 +95,8 @@ class _Request:
     cancel: bool = False
     copying: object = None
     kind: str = "sweep"
+    work_s: float = 0.0            # estimated device time of the whole request (scheduling priority)
+    total_chunks: int = 1
 
 
 class TorchBackend:
@@ -314,6 +316,7 @@ class SweepServer:
                 tw = 2 if launch.trace_mode == "observable" else launch.state_size
                 nbytes += points * launch.num_trace * tw * real
         req = _Request(fut, launch, (nx, ny), int(nbytes), points, points * int(launch.num_steps), kind=kind)
+        req.work_s = _work_estimate(launch, kind, req.point_steps)
         if req.nbytes > self.budget:
             fut._finish(FAILED, error=f"request needs {req.nbytes} bytes, more than the budget {self.budget}")
             return fut
@@ -347,17 +350,25 @@ class SweepServer:
         self.close()
 
     # ------------------------------------------------------------------ server loop
+    def _priority(self, req, now):
+        """Shortest estimated remaining work first, aged by the time since arrival (seconds): a request
+        that has waited longer than its own estimated work goes before any newer one."""
+        left = 1.0 if req.future.state == QUEUED else len(req.chunks) / max(1, req.total_chunks)
+        return (req.work_s * left - (now - req.future.arrival), req.future.id)
+
     def _admit(self):
         while True:
             with self._lock:
                 if not self._queue or len(self._active) >= self.max_inflight:
                     return
-                req = self._queue[0]
+                now = time.perf_counter()
+                req = min(self._queue, key=lambda r: self._priority(r, now))
                 if self._used + req.nbytes > self.budget:
-                    return
-                self._queue.popleft()
+                    return  # the first in line waits for memory; nothing passes it
+                self._queue.remove(req)
             try:
                 req.chunks = deque(self.backend.admit(req, self.chunk_points))
+                req.total_chunks = max(1, len(req.chunks))
             except Exception as exc:  # allocation or upload failure: this request only
                 req.future._finish(FAILED, error=repr(exc))
                 self.stats["failed"] += 1
@@ -370,10 +381,17 @@ class SweepServer:
                 self.stats["max_concurrent"] = max(self.stats["max_concurrent"], len(self._active))
 
     def _dispatch(self):
-        # Round-robin over admitted requests: one chunk each per pass, onto the least-loaded
-        # stream, at most two chunks queued per stream.
+        # One chunk of each admitted request per pass, onto the least-loaded stream, at most two chunks
+        # queued per stream: first the oldest admitted request (so large requests keep progressing
+        # beside small ones), then the others in priority order (least estimated work left first, aged).
         progressed = False
-        for req in list(self._active):
+        now = time.perf_counter()
+        order = sorted(self._active, key=lambda r: self._priority(r, now))
+        if order:
+            oldest = min(self._active, key=lambda r: r.future.id)
+            order.remove(oldest)
+            order.insert(0, oldest)
+        for req in order:
             if req.cancel or not req.chunks or req.copying is not None:
                 continue
             s = min(range(self.nstreams), key=lambda i: self._stream_load[i])
@@ -443,6 +461,24 @@ class SweepServer:
                 return
             if not busy:
                 time.sleep(self.poll_s)
+
+
+_NOMINAL_FLOPS = 2e13  # flop/s that turn the algorithmic work of a request into seconds (priority only)
+
+
+def _work_estimate(launch, kind, point_steps):
+    """Estimated device seconds of a request: point-steps x the algorithmic flops of one point-step
+    (the reduced RHS count, or the density-matrix formula), x 6 for an adjoint (fit) request."""
+    try:
+        frag = launch.entry["frag"]
+        if frag.get("matrix"):
+            per = float(frag["flops_per_point_step"])
+        else:
+            from . import emit
+            per = 4.0 * emit.count_rhs_flops(frag) + 13.0 * frag["state_size"] + 2.0 * emit.count_drive_flops(frag)
+    except Exception:  # launches without emitted code (test doubles, adjoint problems): point-steps alone
+        per = 100.0
+    return point_steps * per * (6.0 if kind == "adjoint" else 1.0) / _NOMINAL_FLOPS
 
 
 def _shape_outputs(req, out):

@@ -56,9 +56,9 @@ class FakeBackend:
         pass
 
 
-def _launch(tag, nx=8, ny=8):
+def _launch(tag, nx=8, ny=8, steps=10):
     return SweepLaunch(entry={}, form="fp64", output_mode="mean", trace_mode=None, state_size=3,
-                       par_x=np.zeros(nx), par_y=np.zeros(ny), consts=[], rho0=None, num_steps=10,
+                       par_x=np.zeros(nx), par_y=np.zeros(ny), consts=[], rho0=None, num_steps=steps,
                        warmup_steps=0, dt=0.1, t_in=0.0, extra={"tag": tag})
 
 
@@ -129,3 +129,16 @@ def test_cancel_queued_and_running_requests():
     assert a.state == CANCELLED and b.state == CANCELLED
     launched_a = [x for x in be.launches if x[0] == 0]
     assert len(launched_a) < 8  # dispatch stopped before all 8 chunks of a
+
+
+def test_small_requests_go_before_large_ones_but_waiting_counts():
+    """Admission takes the queued request with the least estimated work (point-steps x flops), aged by
+    its waiting time; here the slot limit admits one at a time, so the order of admission shows it."""
+    be = FakeBackend(polls=2)
+    # estimates: 64^2 x 1e7 point-steps (0.2 s at the nominal rate) against 4^2 x 1e7 (0.8 ms)
+    big, small = _launch(0, nx=64, ny=64, steps=10**7), _launch(1, nx=4, ny=4, steps=10**7)
+    with SweepServer(backend=be, memory_budget=1 << 20, chunk_points=4096, max_inflight=1) as srv:
+        first = srv.submit_launch(_launch(2, nx=32, ny=32))   # admitted at once (the server is idle)
+        fb, fs = srv.submit_launch(big), srv.submit_launch(small)
+        [f.result(5) for f in (first, fb, fs)]
+    assert fs.admitted_at < fb.admitted_at  # the small request passed the big one queued before it
