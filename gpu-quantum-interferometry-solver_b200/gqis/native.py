@@ -1,7 +1,8 @@
 """The package's fixed native libraries (built in-tree by nvcc for sm_100a).
 
 * ``libgqis_probe.so``  - FMA-pipe and TF32 tensor-core throughput probes (roofline denominators);
-* ``libgqis_render.so`` - phase-space rasteriser kernels (``gqis.render``).
+* ``libgqis_render.so`` - phase-space rasteriser kernels (``gqis.render``);
+* ``libgqis_serve.so``  - native sweep server for C/C++ hosts (``include/gqis_serve.h``).
 
 Model modules (one per model variant) are built separately by ``engine``.
 """
@@ -16,7 +17,8 @@ from pathlib import Path
 from .engine import ARCH_FLAGS, CSRC_DIR, INCLUDE_DIR, PACKAGE_DIR, nvcc_path
 
 BUILD_DIR = PACKAGE_DIR / "_build"
-LIBS = {"gqis_probe": ["gqis_probe.cu"], "gqis_render": ["gqis_render.cu"]}
+LIBS = {"gqis_probe": ["gqis_probe.cu"], "gqis_render": ["gqis_render.cu"], "gqis_serve": ["gqis_serve.cu"]}
+LINK = {"gqis_serve": ["-ldl"]}
 _loaded: dict = {}
 
 
@@ -43,7 +45,7 @@ def build(name, force=False) -> Path:
         return out
     cmd = [nvcc_path(), *ARCH_FLAGS, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
            "-Xcompiler", "-fvisibility=hidden", f"-I{CSRC_DIR}", f"-I{INCLUDE_DIR}",
-           *[str(CSRC_DIR / s) for s in sources], "-o", str(out) + ".tmp", "-lcuda"]
+           *[str(CSRC_DIR / s) for s in sources], "-o", str(out) + ".tmp", "-lcuda", *LINK.get(name, [])]
     proc = subprocess.run(cmd, capture_output=True, text=True)
     if proc.returncode != 0:
         raise RuntimeError(f"nvcc failed for lib{name}.so:\n{proc.stderr[-6000:]}")
