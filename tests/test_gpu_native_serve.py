@@ -82,3 +82,35 @@ def test_native_server_gives_each_request_its_direct_results():
     for k, sw in sweeps.items():
         for n, ref in direct[k].items():
             assert torch.equal(sw.tensors[n], ref), (k, n)
+
+
+@pytest.mark.gpu
+def test_native_server_cancels_a_queued_request():
+    """With one slot, a request queued behind a long adaptive sweep (1024^2 Duffing points) is
+    cancelled before it starts; the running one completes."""
+    import torch
+    from gqis import solver
+    torch.cuda.set_device(0)
+    lib = _lib()
+    lib.gqis_serve_cancel.argtypes = [ctypes.c_void_p, ctypes.c_int64]
+    cases = ref_cases.cases()
+    sweeps = [solver.prepare_sweep(c["api"], *c["args"], **c["kwargs"])
+              for c in (cases["duffing_tsit5a_full_final"], cases["c2_fp64_mean_sub32"])]
+    server = ctypes.c_void_p()
+    assert lib.gqis_serve_open(0, 2, 1, 1 << 16, 0, ctypes.byref(server)) == 0
+    try:
+        ids = []
+        for sw in sweeps:
+            rid = ctypes.c_int64()
+            assert lib.gqis_serve_submit(server, str(sw.module.path).encode(), ctypes.addressof(sw.desc), 0,
+                                         ctypes.byref(rid)) == 0
+            ids.append(rid.value)
+        assert lib.gqis_serve_cancel(server, ids[1]) == 0
+        states = []
+        for rid in ids:
+            state = ctypes.c_int32()
+            assert lib.gqis_serve_wait(server, rid, 300.0, ctypes.byref(state)) == 0
+            states.append(state.value)
+        assert states == [2, 4]  # DONE, CANCELLED
+    finally:
+        assert lib.gqis_serve_close(server) == 0
