@@ -22,6 +22,7 @@ import os
 import sys
 import time
 import warnings
+from contextlib import contextmanager
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -62,9 +63,28 @@ MATRIX_FORM_FROM = 8  # rhs_form="auto" switches to the density-matrix kernels f
 # the tensor cores 11 ms vs 65 ms; the reduced form stays faster at N = 4)
 
 
+@contextmanager
+def _nvtx(name):
+    """An NVTX range around a stage of a call (seen by Nsight Systems and Nsight Compute), when torch
+    has a CUDA device; otherwise nothing."""
+    try:
+        import torch
+        on = torch.cuda.is_available()
+    except ImportError:
+        on = False
+    if on:
+        torch.cuda.nvtx.range_push(name)
+    try:
+        yield
+    finally:
+        if on:
+            torch.cuda.nvtx.range_pop()
+
+
 def _compile_rhs(*args, **kwargs):
     """Indirection so tests can count symbolic preparations."""
-    return _compile_rhs_impl(*args, **kwargs)
+    with _nvtx("gqis.compile_rhs"):
+        return _compile_rhs_impl(*args, **kwargs)
 
 
 def compile_lindblad_rhs(H, Drive, Col_Ops, mean_operator, sweep_symbols, *, const_values=None,
@@ -125,7 +145,8 @@ def _load_kernel(entry):
     """Build (nvcc, disk-cached) and load the module of a kernel-cache entry."""
     if entry.get("module") is None:
         from . import engine
-        entry["module"] = engine.load_module(entry["source"], extra_flags=entry.get("flags", ()))
+        with _nvtx("gqis.build_module"):
+            entry["module"] = engine.load_module(entry["source"], extra_flags=entry.get("flags", ()))
     return entry["module"]
 
 
@@ -309,7 +330,10 @@ def prepare_sweep(api, *args, point_begin=0, point_count=None, **kwargs):
 def _to_output(tensor, return_device):
     if tensor is None:
         return None
-    return tensor if return_device else tensor.cpu().numpy()
+    if return_device:
+        return tensor
+    with _nvtx("gqis.copy_out"):
+        return tensor.cpu().numpy()
 
 
 def _all_finite(x):
@@ -577,10 +601,11 @@ def _solve_symbolic_system(H, Drive, Col_Ops, mean_operator, tlist,
     # ---- 1) symbolic preparation
     if use_matrix:
         from . import matrix_form
-        compiled, rhs_status = matrix_form.compile_matrix_model(
-            H, Drive, Col_Ops, mean_operator, sweep_symbols=tuple(var_arrays), const_values=const_values,
-            runtime_consts=runtime_consts, keep_symbolic_consts=keep_symbolic_consts,
-            auto_runtime_consts=auto_runtime_consts, rho0=rho0, reuse=RHSreuse)
+        with _nvtx("gqis.compile_matrix_model"):
+            compiled, rhs_status = matrix_form.compile_matrix_model(
+                H, Drive, Col_Ops, mean_operator, sweep_symbols=tuple(var_arrays), const_values=const_values,
+                runtime_consts=runtime_consts, keep_symbolic_consts=keep_symbolic_consts,
+                auto_runtime_consts=auto_runtime_consts, rho0=rho0, reuse=RHSreuse)
         if rhs_form == "auto" and not matrix_form.tensor_core_blockers(compiled, form):
             tensor_cores = True  # FP32 sweeps of N = 16 .. 32 run on the tensor cores
     elif compiled_rhs is None:
@@ -614,7 +639,8 @@ def _solve_symbolic_system(H, Drive, Col_Ops, mean_operator, tlist,
     elif RHSreuse and ekey in compiled.emitted:
         frag, stages["emit_s"] = compiled.emitted[ekey], 0.0
     else:
-        frag = emit.emit_model(compiled, uses_rho0_values)
+        with _nvtx("gqis.emit"):
+            frag = emit.emit_model(compiled, uses_rho0_values)
         if RHSreuse:
             compiled.emitted[ekey] = frag
         stages["emit_s"] = time.time() - t0
@@ -689,7 +715,8 @@ def _solve_symbolic_system(H, Drive, Col_Ops, mean_operator, tlist,
     _load_kernel(entry)
     stage_build = time.time() - t_build
     rhs_stage_s = time.time() - t_total
-    results, trace, counts, gpu_s = _device_run(launch)
+    with _nvtx("gqis.sweep"):
+        results, trace, counts, gpu_s = _device_run(launch)
 
     # ---- 5) outputs
     cplx = mode in ("mean", "final")

@@ -9,6 +9,7 @@ import warnings
 from unittest.mock import patch
 
 import numpy as np
+import pytest
 import sympy as sp
 
 import gqis.solver as core
@@ -325,3 +326,22 @@ def test_repeated_call_skips_model_preparation_and_follows_mutated_matrices():
         changed, status = rhs.compile_rhs(H, A * sp.cos(t), ops, sp.diag(0, 1), **call)
         assert status == "miss" and changed is not first
     rhs._RHS_CODE_CACHE.clear()
+
+
+def test_non_finite_output_raises_unless_ignored():
+    """A non-finite point in the returned map raises RuntimeError (gqis/solver.py:2351-2362 of the
+    reference); ignore_non_finite_output returns the map with it. The failure is made on the host."""
+    eps, A, t = sp.symbols("eps A t", real=True)
+    H = sp.Matrix([[eps / 2, 0.5], [0.5, -eps / 2]])
+    call = ((H, A * sp.cos(t), [0.1 * sp.Matrix([[0, 1], [0, 0]])], sp.diag(0, 1), np.linspace(0, 1, 5)),
+            dict(var_arrays={eps: np.linspace(-1, 1, 4), A: np.linspace(0, 1, 3)}, fp64=True))
+
+    def values(launch):
+        v = np.zeros((len(launch.par_x) * len(launch.par_y), 2))
+        v[5, 0] = np.nan
+        return v
+    with fake_device(values):
+        with pytest.raises(RuntimeError, match="Non-finite"):
+            mesolve_2D(*call[0], **call[1])
+        out = mesolve_2D(*call[0], **call[1], ignore_non_finite_output=True)
+    assert out.shape == (4, 3) and int(np.isnan(out.real).sum()) == 1 and np.isnan(out.real[1, 2])

@@ -1,0 +1,39 @@
+"""Failures made on the host, checked on the GPU (no device fault, trap or hang is involved): an
+adaptive substep cap too small for the tolerance marks points NaN and the call raises; a NaN sweep
+parameter poisons only its own points."""
+
+import numpy as np
+import pytest
+
+import ref_cases
+from test_support_calls import duffing_case
+
+
+@pytest.mark.gpu
+def test_adaptive_substep_cap_marks_points_nan_and_raises():
+    import gqis
+    _, args, kwargs = duffing_case(solver="tsit5a")
+    kwargs = dict(kwargs, adaptive_options=dict(kwargs["adaptive_options"], max_substeps=1))
+    with pytest.raises(RuntimeError, match="Non-finite"):
+        gqis.odesolve_2D(*args, **kwargs)
+    out = gqis.odesolve_2D(*args, **kwargs, ignore_non_finite_output=True)
+    final = out[0] if isinstance(out, tuple) else out
+    assert np.isnan(np.asarray(final, dtype=np.float64)).any()
+
+
+@pytest.mark.gpu
+def test_nan_parameter_poisons_only_its_points():
+    import gqis
+    case = ref_cases.cases()["c2_fp64_mean_sub32"]
+    clean = gqis.mesolve_2D(*case["args"], **case["kwargs"])
+    va = dict(case["kwargs"]["var_arrays"])
+    first = list(va)[0]
+    axis = np.array(va[first], dtype=np.float64)
+    axis[5] = np.nan
+    va[first] = axis
+    bad = dict(case["kwargs"], var_arrays=va)
+    with pytest.raises(RuntimeError, match="Non-finite"):
+        gqis.mesolve_2D(*case["args"], **bad)
+    out = gqis.mesolve_2D(*case["args"], **bad, ignore_non_finite_output=True)
+    assert np.isnan(out[5].real).all()
+    np.testing.assert_array_equal(np.delete(out, 5, axis=0), np.delete(clean, 5, axis=0))
