@@ -11,7 +11,8 @@
  * until the request has ended (DONE, FAILED or CANCELLED). The server allocates only its own
  * streams, events and a small array of work counters for adaptive chunks. All functions return
  * a GQIS_* status; gqis_serve_last_error() describes the last failure of the calling thread.
- * A server handle may be used from several host threads.
+ * A server handle may be used from several host threads. Ended requests stay queryable (state,
+ * error text) until gqis_serve_close, a few hundred bytes each.
  */
 #ifndef GQIS_SERVE_H
 #define GQIS_SERVE_H
