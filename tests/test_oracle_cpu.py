@@ -89,3 +89,26 @@ def test_c_oracle_adaptive_dop853_agrees_with_scipy():
                             (0.0, 500.0), d["y0_values"][i, j], method="DOP853", rtol=1e-12, atol=1e-13)
             assert np.max(np.abs(sol.y[:, -1] - final[i, j])) < 5e-6
     assert counts[..., 0].min() > 100
+
+
+@pytest.mark.parametrize("case", ["rabi", "commuting", "mean", "decay"])
+def test_matrix_oracle_known_answers(case):
+    """The density-matrix oracle reproduces the analytic answers the GPU known-answer tests use."""
+    import test_support_calls as ka
+    args, kw = {"rabi": lambda: ka.rabi_call("rk4", True), "commuting": lambda: ka.commuting_call("rk4"),
+                "mean": lambda: ka.commuting_call("rk4", "mean"), "decay": ka.decay_call}[case]()
+    H, Drive, Col_Ops, O, tlist = args
+    rho0 = np.array(kw["rho0"].tolist(), dtype=complex) if "rho0" in kw else None
+    model = lindblad_oracle.MatrixModel(H, Drive, Col_Ops, O, kw["var_arrays"])
+    out = lindblad_oracle.rk4_sweep(model, tlist, output_mode=kw["output_mode"], rho0=rho0)
+    x = np.linspace(0.5, 2.0, 4)
+    if case == "rabi":
+        got, exact = out[:, 0, 0], np.cos(x * np.pi / 2) ** 2
+    elif case == "commuting":
+        got, exact = out[:, 0, 0], np.cos(x * np.sin(5.0) / 2) ** 2
+    elif case == "mean":
+        got = out.real[:, 0]
+        exact = np.mean(np.sin(x[:, None] * np.sin(tlist[1:]) / 2) ** 2, axis=1)
+    else:
+        got, exact = out[..., 0], 1 - np.exp(-0.3 * 4.0)
+    assert np.max(np.abs(got - exact)) <= 1e-9

@@ -5,8 +5,10 @@ loads these modules instead of compiling them.
 """
 
 import numpy as np
+import sympy as sp
 
 import ref_cases
+from gqis.cuda_solvers import available_solvers, get_solver_spec
 
 ADAPTIVE_OPTIONS = {"step_rtol": 1e-8, "step_atol": 1e-10, "max_substeps": 4000, "count_steps": True}
 
@@ -139,4 +141,61 @@ def adjoint_problems():
            (args, dict(kwargs, params=list(params), output="final"))]
     args, kwargs, params = qubit_fit_model(side=(256, 256), steps=4000, duration=200.0)
     out.append((args, dict(kwargs, params=list(params[:3]))))
+    return out
+
+
+# analytic known-answer cases (tests/test_gpu_known_answers.py)
+FIXED = [s for s in available_solvers() if not get_solver_spec(s).adaptive]
+ADAPTIVE = [s for s in available_solvers() if get_solver_spec(s).adaptive]
+SX = sp.Matrix([[0, 1], [1, 0]])
+SZ = sp.Matrix([[1, 0], [0, -1]])
+
+
+def rabi_call(solver, fp64):
+    Om, eps, Drive = sp.symbols("Omega eps Drive", real=True)
+    kw = dict(var_arrays={Om: np.linspace(0.5, 2.0, 4), eps: np.array([0.0])}, output_mode="final_rho",
+              solver=solver)
+    kw.update(dict(fp64=True) if fp64 else dict(precision="fp32"))
+    if solver == "anas5":
+        kw["solver_frequency"] = 1.0
+    return (Drive / 2 * SX + eps / 2 * SZ, Om, [], sp.diag(0, 1), np.linspace(0.0, np.pi, 801)), kw
+
+
+def commuting_call(solver, output_mode="final_rho"):
+    A, eps, Drive, t = sp.symbols("A eps Drive t", real=True)
+    kw = dict(var_arrays={A: np.linspace(0.5, 2.0, 4), eps: np.array([0.0])}, output_mode=output_mode,
+              solver=solver, fp64=True)
+    if solver == "anas5":
+        kw["solver_frequency"] = 1.0
+    if get_solver_spec(solver).adaptive:
+        kw["adaptive_options"] = {"step_rtol": 1e-12, "step_atol": 1e-12, "max_substeps": 4000}
+    return (Drive / 2 * SX + eps / 2 * SZ, A * sp.cos(t), [], sp.diag(0, 1), np.linspace(0.0, 5.0, 2001)), kw
+
+
+def decay_call():
+    eps, Drive = sp.symbols("eps Drive", real=True)
+    sm = sp.Matrix([[0, 1], [0, 0]])
+    kw = dict(var_arrays={eps: np.linspace(-1.0, 1.0, 3)}, output_mode="final_rho", fp64=True,
+              rho0=sp.diag(0, 1))
+    return (Drive / 2 * SZ, eps, [sp.sqrt(0.3) * sm], sp.diag(0, 1), np.linspace(0.0, 4.0, 801)), kw
+
+
+def ode_call():
+    x, y, t, k = sp.symbols("x y t k", real=True)
+    kw = dict(var_arrays={k: np.linspace(0.5, 2.0, 4)}, fp64=True, output_mode="final")
+    return ([-k * x, t], [x, y], [1.0, 0.0], np.linspace(0.0, 2.0, 1001)), kw
+
+
+def known_answer_calls():
+    """(api, args, kwargs) of every known-answer launch."""
+    out = []
+    for s in FIXED:
+        for fp64 in (True, False):
+            out.append(("mesolve_2D",) + rabi_call(s, fp64))
+        out.append(("mesolve_2D",) + commuting_call(s))
+    for s in ADAPTIVE:
+        out.append(("mesolve_2D",) + commuting_call(s))
+    out.append(("mesolve_2D",) + commuting_call("rk4", "mean"))
+    out.append(("mesolve_2D",) + decay_call())
+    out.append(("odesolve_2D",) + ode_call())
     return out
