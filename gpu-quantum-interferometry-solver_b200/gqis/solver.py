@@ -1030,8 +1030,9 @@ def _calibrate_timestep(args, settings, base_steps, duration):
         scale = 1.0 / (1.0 - (x / fine_x) ** order)
         diff = np.abs(fine - coarse) * scale
         mag = np.abs(fine)
-        rec.update(rms=float(np.sqrt(np.mean(diff**2))), max=float(np.max(diff)))
-        rms_lim = settings["rms_atol"] + settings["rms_rtol"] * float(np.sqrt(np.mean(mag**2)))
+        with np.errstate(over="ignore"):  # a diverging candidate's squares overflow to inf: rejected
+            rec.update(rms=float(np.sqrt(np.mean(diff**2))), max=float(np.max(diff)))
+            rms_lim = settings["rms_atol"] + settings["rms_rtol"] * float(np.sqrt(np.mean(mag**2)))
         max_lim = settings["max_atol"] + settings["max_rtol"] * float(np.max(mag))
         ok = ((not settings["check_rms"] or rec["rms"] <= rms_lim)
               and (not settings["check_max"] or rec["max"] <= max_lim))
