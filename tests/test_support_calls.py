@@ -1,7 +1,7 @@
 """Model-module variants used by GPU tests beyond the reference cases (prebuilt by build()).
 
-Not a test module itself: ``__graft_entry__.build()`` imports ``calls()`` so that the GPU box
-loads these modules instead of compiling them.
+Not a test module itself: ``__graft_entry__.build()`` imports ``calls()`` so that the GPU tests
+load these modules instead of compiling them.
 """
 
 import numpy as np
