@@ -158,6 +158,13 @@ def cpu_reference(steps=1, sample="c2_fp64_mean_sub64"):
             "sample": "16x16 strided subgrid, 800 RK4 steps, NumPy density-matrix oracle (one core)"}
 
 
+def four_level_config(side, nsteps, ws):
+    """The four-level workload's ``config``, shared by both arms (the reference arm times a sample of it)."""
+    return {"workload": f"four-level Lindblad interferogram, {side}x{side} (eps, A) grid per GPU, "
+                        f"RK4 {nsteps} steps on [0, {DURATION * nsteps / NSTEPS:g}], mean <|3><3|>",
+            "points_per_gpu": side * side, "rk4_steps": nsteps, "parallelism": f"sweep shards x{ws}"}
+
+
 def run_reference(args):
     ws, rank, _ = _dist()
     if rank != 0:
@@ -169,7 +176,7 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.median(times),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": f"four-level Lindblad RK4 sweep, {ref['sample']}"},
+            "data": "synthetic", "config": four_level_config(args.side, args.nsteps, args.gpus),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": ref["cores"], "kind": ref["kind"],
                              "sample": ref["sample"]},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -262,11 +269,9 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms32, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"four-level Lindblad interferogram, {side}x{side} (eps, A) grid per GPU, "
-                                   f"RK4 {ksteps} steps on [0, {DURATION * nsteps / NSTEPS:g}], mean <|3><3|>",
-                       "points_per_gpu": points, "rk4_steps": ksteps, "parallelism": f"sweep shards x{ws}",
-                       "l2": "flushed (256 MiB write) between timed launches",
-                       "form": "FP32 state/RHS, FP64 time + drive phase + compensated average"},
+            "config": dict(four_level_config(side, ksteps, ws),
+                           l2="flushed (256 MiB write) between timed launches",
+                           form="FP32 state/RHS, FP64 time + drive phase + compensated average"),
             "plain_fp64": {"value": total_units / (ms64 / 1e3), "ms_per_step": ms64},
             "speedup_vs_plain_fp64": ms64 / ms32,
             "max_abs_err_vs_fp64": err,
