@@ -145,9 +145,10 @@ def _solve_ode_system(rhs, state_symbols, y0, tlist, *, var_arrays, const_values
                       observable, output_mode, y0_values, runtime_consts, keep_symbolic_consts,
                       solver, fp64, return_time_trace, time_trace_every, t_in, return_device,
                       calibrate_timesteps, **option_set):
-    from .solver import CompiledRHS, _solve_symbolic_system
+    from .solver import CompiledRHS, _check_sweep_arrays_nonempty, _solve_symbolic_system
     if tlist is None:
         raise TypeError("odesolve_2D needs tlist.")
+    _check_sweep_arrays_nonempty(var_arrays)
     if output_mode not in {"mean", "final"}:
         raise ValueError("output_mode must be 'mean' or 'final'.")
     if y0 is not None and y0_values is not None:

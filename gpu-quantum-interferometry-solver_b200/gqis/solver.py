@@ -441,6 +441,14 @@ def _resolve_precision(precision, fp64):
     return p
 
 
+def _check_sweep_arrays_nonempty(var_arrays):
+    """Reject a sweep array without values: its grid has zero points, which the launch rejects
+    (the module's descriptor check), so say so before any derivation or compile."""
+    for sym, arr in (var_arrays or {}).items():
+        if (arr.numel() if hasattr(arr, "numel") else np.size(arr)) == 0:
+            raise ValueError(f"The sweep array of {sym} is empty; every sweep array needs at least one value.")
+
+
 def _solve_symbolic_system(H, Drive, Col_Ops, mean_operator, tlist,
                            var_arrays=None, const_values=None, kernel_template_file=None, *,
                            RHSreuse=True, runtime_consts=None, keep_symbolic_consts=None,
@@ -513,6 +521,7 @@ def _solve_symbolic_system(H, Drive, Col_Ops, mean_operator, tlist,
         raise ValueError("var_arrays or rho0_var_arrays must contain at least one sweep array (ParX).")
     if len(var_arrays) > 2:
         raise ValueError("Only 2 total sweep arrays are supported across var_arrays and rho0_var_arrays.")
+    _check_sweep_arrays_nonempty(var_arrays)
     if compiled_rhs is None:
         if H is None or Drive is None or Col_Ops is None or mean_operator is None:
             raise TypeError("Give H, Drive, Col_Ops and mean_operator, or a CompiledRHS.")

@@ -345,3 +345,18 @@ def test_non_finite_output_raises_unless_ignored():
             mesolve_2D(*call[0], **call[1])
         out = mesolve_2D(*call[0], **call[1], ignore_non_finite_output=True)
     assert out.shape == (4, 3) and int(np.isnan(out.real).sum()) == 1 and np.isnan(out.real[1, 2])
+
+
+def test_empty_sweep_axis_is_rejected_before_any_compile():
+    """A sweep array without values gives a zero-point grid, which the launch rejects; the front end says
+    so before deriving or compiling anything (for either axis, and for odesolve_2D)."""
+    eps, A, x, k = sp.symbols("eps A x k", real=True)
+    H = eps / 2 * sp.Matrix([[1, 0], [0, -1]]) + sp.Symbol("Drive", real=True) / 2 * sp.Matrix([[0, 1], [1, 0]])
+    tl = np.linspace(0.0, 1.0, 11)
+    with fake_device() as dev:
+        for va in ({eps: np.array([]), A: np.linspace(0, 1, 3)}, {eps: np.linspace(0, 1, 3), A: []}):
+            with pytest.raises(ValueError, match="is empty"):
+                mesolve_2D(H, A, [], sp.diag(0, 1), tl, var_arrays=va, fp64=True)
+        with pytest.raises(ValueError, match="sweep array of k is empty"):
+            odesolve_2D([-k * x], [x], [1.0], tl, var_arrays={k: np.zeros(0)}, fp64=True)
+        assert not dev.sources and not dev.launches
