@@ -246,6 +246,79 @@ class OdeApiTests(unittest.TestCase):
         self.assertEqual(steps_for(512, 2), 76)
         self.assertEqual(steps_for(512, 0), 512)
 
+    def _calibrated_with(self, value_of, **kwargs):
+        """Calibration report of a mesolve_2D call whose uncalibrated runs return ``value_of(call)`` at
+        every point (a 4-point sweep, 16 starting steps on [0, 1])."""
+        real = core._solve_symbolic_system
+
+        def run(**call):
+            if call.get("calibrate_timesteps"):
+                return real(**call)
+            nx, ny = (len(v) for v in (list(call["var_arrays"].values()) + [[0.0]])[:2])
+            out = np.full((nx, ny), value_of(call), dtype=complex)
+            return (out, {}) if call.get("return_timing_info") else out
+
+        core._TIMESTEP_CALIBRATION_CACHE.clear()
+        with patch.object(core, "_solve_symbolic_system", side_effect=run):
+            _, info = real(H=sp.eye(2), Drive=sp.Integer(0), Col_Ops=[], mean_operator=sp.eye(2),
+                           tlist=np.linspace(0, 1, 17), var_arrays={self.a: np.ones(4)},
+                           return_timing_info=True, **kwargs)
+        return info["timestep_calibration"]
+
+    def test_timestep_calibration_mean_uses_first_order_estimate(self):
+        """tests/test_ode_api.py:293-300 of the reference: a time average whose error is 1/steps is
+        extrapolated as first order (1e-3 needs 1024 steps); the same error read as RK4's fourth
+        order would pass at 724."""
+        limits = dict(rms_atol=1e-3, max_atol=1e-2)
+        def value(call):
+            return 0.3 + 1.0 / (len(call["tlist"]) - 1)
+        self.assertEqual(self._calibrated_with(value, output_mode="mean", calibrate_timesteps=limits)["steps"], 1024)
+        self.assertEqual(self._calibrated_with(value, output_mode="final", calibrate_timesteps=limits)["steps"], 724)
+
+    def test_tsit5a_calibration_scales_both_tolerances(self):
+        """tests/test_ode_api.py:302-313: an error of 7 x the step tolerance meets 1e-3 from 1.4e-4 down;
+        the search moves by decades from either side and keeps the rtol / atol ratio; output times
+        never change."""
+        def value(call):
+            self.assertEqual(len(call["tlist"]), 17)
+            o = call["adaptive_options"]
+            return 0.3 + 7.0 * max(o["step_rtol"], o["step_atol"])
+        for start in (1e-5, 1e-2):
+            r = self._calibrated_with(value, solver="tsit5a", calibrate_timesteps=dict(rms_atol=1e-3, max_atol=1e-2),
+                                      adaptive_options=dict(step_rtol=start, step_atol=start / 5))
+            self.assertAlmostEqual(r["step_tol"], 1e-4)
+            self.assertAlmostEqual(r["step_rtol"], 1e-4)
+            self.assertAlmostEqual(r["step_atol"], 2e-5)
+
+    def test_tsit5a_calibration_stops_at_max_substeps(self):
+        """tests/test_ode_api.py:315-322: tolerances below 1e-6 exceed max_substeps (NaN points); the
+        search stops at 1e-6, warns and reports the status."""
+        def value(call):
+            tol = call["adaptive_options"]["step_rtol"]
+            return np.nan if tol < 0.99e-6 else 0.3 + 1e3 * tol
+        with self.assertWarnsRegex(RuntimeWarning, "max_substeps"):
+            r = self._calibrated_with(value, solver="tsit5a", calibrate_timesteps=dict(rms_atol=1e-3, max_atol=1e-2))
+        self.assertAlmostEqual(r["step_tol"], 1e-6)
+        self.assertEqual(r["details"]["status"], "max_substeps")
+
+    def test_timestep_calibration_key_includes_max_steps_and_reuses_full_grid(self):
+        """tests/test_ode_api.py:228-247: max_steps is part of the cache key; a full-grid test reuses its
+        final run and skips bisection (two launches), unless full_grid_bisection asks for it. Launches
+        are counted on the device seam: every candidate here comes from one prepared launch."""
+        with patch.object(core, "_calibrate_timestep", wraps=core._calibrate_timestep) as calibrate:
+            self.solve(calibrate_timesteps=dict(rms_atol=1e-4, sample_stride=1))
+            self.solve(calibrate_timesteps=dict(rms_atol=1e-4, sample_stride=1, max_steps=2**10))
+            self.assertEqual(calibrate.call_count, 2)
+
+        def launches(**settings):
+            before = len(self.dev.launches)
+            self.solve(calibrate_timesteps=dict(rms_atol=1e-4, sample_stride=1, reset=True, **settings))
+            return len(self.dev.launches) - before
+        self.assertEqual(launches(bisection_steps=0), 2)
+        self.assertEqual(launches(bisection_steps=2), 2)
+        self.assertEqual(launches(), 2)
+        self.assertGreater(launches(full_grid_bisection=True), 2)
+
     def test_timestep_calibration_defaults_differ_for_lindblad_and_ode(self):
         lindblad = core._timestep_calibration_settings(True)
         ode = core._timestep_calibration_settings(True, ode=True)
