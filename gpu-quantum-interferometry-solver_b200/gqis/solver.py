@@ -673,8 +673,11 @@ def _solve_symbolic_system(H, Drive, Col_Ops, mean_operator, tlist,
                                             trace=trace_mode == "observable")
                   if use_matrix
                   else engine.module_source(frag, spec, form, mode, trace_mode, unroll))
+        # `unroll` (the reference's "#pragma unroll on the solver's vector loops", gqis/solver.py:1821)
+        # is validated and reported but builds the same module: the templates unroll every loop over
+        # the state, which is what keeps the state in registers.
         entry = {"source": source,
-                 "module": None, "flags": flags + (("-DGQ_FULL_UNROLL=1",) if unroll else ()),
+                 "module": None, "flags": flags,
                  "frag": frag, "spec": spec, "compiled": compiled}
         if RHSreuse:
             _KERNEL_CACHE[kkey] = entry

@@ -60,6 +60,9 @@ class OdeApiTests(unittest.TestCase):
         self.solve(t_in=5.0, return_time_trace=True)
         self.assertEqual(len(self.codes), 1)
         self.assertEqual(self.dev.launches[-1].t_in, 5.0)
+        self.solve(t_in=0.0, return_time_trace=True)  # zero and non-zero offsets share one module
+        self.assertEqual(len(self.codes), 1)
+        self.assertEqual(self.dev.launches[-1].t_in, 0.0)
 
     def test_observable_and_fp64(self):
         result, trace, times = self.solve(observable=(self.x + self.y)**2 + sp.I * (self.x + self.y)**3 + self.t,
@@ -433,3 +436,19 @@ def test_empty_sweep_axis_is_rejected_before_any_compile():
         with pytest.raises(ValueError, match="sweep array of k is empty"):
             odesolve_2D([-k * x], [x], [1.0], tl, var_arrays={k: np.zeros(0)}, fp64=True)
         assert not dev.sources and not dev.launches
+
+
+def test_forced_unrolling_is_reported_and_builds_the_same_module():
+    """After the reference's tests/test_gpu_solver.py:59-73: ``unroll=True`` is accepted and reported in
+    the timing dictionary. The templates already unroll every loop over the state (which keeps it
+    in registers), so both settings build one module with the same flags."""
+    d = sp.Symbol("dummy", real=True)
+    model = (sp.zeros(2), sp.Integer(0), [], sp.eye(2), np.linspace(0.0, 1.0, 5))
+    with fake_device() as dev:
+        _, timing = mesolve_2D(*model, var_arrays={d: np.array([0.0])}, output_mode="final_rho", unroll=True,
+                               return_timing_info=True)
+        assert timing["solver"] == "rk4" and timing["unroll"] is True
+        flags = [core.prebuild("mesolve_2D", *model, var_arrays={d: np.array([0.0])}, output_mode="final_rho",
+                               unroll=u, source_only=True) for u in (False, True)]
+        assert flags[0] == flags[1]
+        assert len(set(dev.sources)) == 1
