@@ -60,3 +60,16 @@ def test_option_groups_merge_and_reject_conflicts():
     with pytest.raises(ValueError, match="Unknown codegen option"):
         apply_option_groups(f, dict(args), {"codegen": {"fp64": True}})
     assert "precision" in OPTION_GROUPS["solver_options"]
+
+
+def test_api_reference_documents_every_parameter():
+    """After the reference's tests/test_package.py:42-46: the API reference names every parameter of
+    both entry points."""
+    import inspect
+    from pathlib import Path
+
+    from gqis import mesolve_2D, odesolve_2D
+    doc = (Path(__file__).resolve().parents[1] / "API.md").read_text(encoding="utf-8")
+    for func in (mesolve_2D, odesolve_2D):
+        missing = [name for name in inspect.signature(func).parameters if f"`{name}`" not in doc]
+        assert missing == [], (func.__name__, missing)
