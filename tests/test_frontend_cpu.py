@@ -73,3 +73,19 @@ def test_api_reference_documents_every_parameter():
     for func in (mesolve_2D, odesolve_2D):
         missing = [name for name in inspect.signature(func).parameters if f"`{name}`" not in doc]
         assert missing == [], (func.__name__, missing)
+
+
+def test_package_import_needs_no_cupy_or_triton():
+    """After the reference's tests/test_package.py:15-39 (import without CuPy): the package and every
+    submodule import in a fresh process without a GPU, and load neither CuPy nor Triton."""
+    import subprocess
+    import sys
+    from pathlib import Path
+
+    pkg = Path(__file__).resolve().parents[1] / "gpu-quantum-interferometry-solver_b200"
+    code = ("import sys; sys.path.insert(0, %r)\n"
+            "import gqis, gqis.solver, gqis.serving, gqis.adjoint, gqis.render, gqis.shard, gqis.matrix_form\n"
+            "bad = sorted(m for m in sys.modules if m.split('.')[0] in ('cupy', 'triton'))\n"
+            "assert not bad, bad\n") % str(pkg)
+    proc = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
+    assert proc.returncode == 0, proc.stderr[-2000:]
