@@ -452,3 +452,24 @@ def test_forced_unrolling_is_reported_and_builds_the_same_module():
                                unroll=u, source_only=True) for u in (False, True)]
         assert flags[0] == flags[1]
         assert len(set(dev.sources)) == 1
+
+
+def test_calibrated_trace_keeps_the_sample_times_of_the_given_grid():
+    """After the reference's tests/test_gpu_solver.py:206-228: when calibration refines the step, the
+    trace is still sampled at the times of the supplied grid (stride and offset scaled with it)."""
+    eps, A, t = sp.symbols("eps A t", real=True)
+    H = eps / 2 * sp.Matrix([[1, 0], [0, -1]]) + sp.Symbol("Drive", real=True) / 2 * sp.Matrix([[0, 1], [1, 0]])
+    period = 2 * np.pi
+    call = dict(var_arrays={eps: np.linspace(-1, 1, 4), A: np.linspace(0.1, 1, 3)}, output_mode="final",
+                return_time_trace=True, time_trace_every=8, fp64=True)
+    model = (H, A * sp.cos(t), [], sp.diag(0, 1), np.linspace(0.0, period, 33))
+    with fake_device(values=lambda launch: 0.3 + 3e4 / launch.num_steps ** 4) as dev:
+        _, plain_trace, plain_times = mesolve_2D(*model, **call)
+        _, trace, times, info = mesolve_2D(*model, **call, calibrate_timesteps=dict(rms_atol=1e-3, max_atol=1e-2),
+                                           return_timing_info=True)
+        final = dev.launches[-1]
+    assert info["timestep_calibration"]["steps"] > 32  # the grid was refined
+    np.testing.assert_allclose(plain_times, (np.arange(4) * 8 + 1) * period / 32)
+    np.testing.assert_allclose(times, plain_times, rtol=1e-12)
+    assert trace.shape == plain_trace.shape
+    assert final.num_steps % 32 == 0 and final.trace_stride == 8 * final.num_steps // 32
