@@ -136,6 +136,7 @@ class ModelModule:
         self._info = None
 
     def info(self):
+        """The module's ``gqis_model_info`` (state size, solver, output mode, launch shape), read once."""
         from . import abi
         if self._info is None:
             info = abi.ModelInfo()
@@ -145,6 +146,8 @@ class ModelModule:
         return self._info
 
     def launch(self, desc, stream_handle):
+        """``gqis_sweep_launch`` of a filled descriptor on a CUDA stream handle; raises on a non-OK
+        status with the module's error text."""
         from . import abi
         rc = self.lib.gqis_sweep_launch(ctypes.byref(desc), ctypes.c_void_p(stream_handle))
         abi.check(rc, self.lib)

@@ -31,6 +31,7 @@ def _digest(sources):
 
 
 def lib_path(name) -> Path:
+    """In-tree path of the fixed library ``lib<name>.so``."""
     return BUILD_DIR / f"lib{name}.so"
 
 

@@ -43,9 +43,12 @@ class SweepFuture:
         self._event = threading.Event()
 
     def done(self):
+        """True once the request has ended (done, failed or cancelled)."""
         return self._event.is_set()
 
     def result(self, timeout=None):
+        """Wait for the request and return its results; raises if it failed, was cancelled or did
+        not end within ``timeout`` seconds."""
         if not self._event.wait(timeout):
             raise TimeoutError(f"request {self.id} not finished within {timeout} s")
         if self.state == FAILED:
@@ -56,6 +59,7 @@ class SweepFuture:
 
     @property
     def latency(self):
+        """Seconds from submission to completion (None while the request runs)."""
         return None if self.finished_at is None else self.finished_at - self.arrival
 
     def _finish(self, state, result=None, error=None):
@@ -301,6 +305,8 @@ class SweepServer:
         return self.submit_launch(fit, nbytes=nbytes, kind="adjoint")
 
     def submit_launch(self, launch, nbytes=None, kind="sweep"):
+        """Queue a prepared launch; ``nbytes`` is its device memory for admission (estimated from the
+        launch when None). A request larger than the whole budget fails at once."""
         rid = next(self._ids)
         fut = SweepFuture(rid, time.perf_counter())
         nx = len(launch.par_x)
@@ -326,6 +332,8 @@ class SweepServer:
         return fut
 
     def cancel(self, fut):
+        """Cancel a request: a queued one ends at once, a running one after its chunks in flight.
+        Returns False if the request has already ended."""
         with self._lock:
             for req in list(self._queue):
                 if req.future is fut:
@@ -340,6 +348,8 @@ class SweepServer:
         return False
 
     def close(self, timeout=60.0):
+        """Stop accepting work once the queue is drained: the scheduler thread finishes every queued and
+        running request, then exits; waits up to ``timeout`` seconds for it."""
         self._stop = True
         self._thread.join(timeout)
 

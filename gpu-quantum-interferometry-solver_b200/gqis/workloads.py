@@ -37,6 +37,8 @@ def _axis(lo, hi, full, side):
 
 
 def two_level(side=None, full=64, steps=4000, duration=200.0):
+    """The driven-qubit model of the module docstring on a ``full``-point axis pair (``side``: a
+    strided subgrid of it)."""
     eps, A, Delta, Drive, t = sp.symbols("eps A Delta Drive t", real=True)
     sz = sp.Matrix([[1, 0], [0, -1]])
     sx = sp.Matrix([[0, 1], [1, 0]])
@@ -52,11 +54,14 @@ def two_level(side=None, full=64, steps=4000, duration=200.0):
 
 
 def four_level_couplings(seed=0):
+    """The three nearest-neighbour couplings of the four-level model, U(0.1, 1), six digits."""
     rng = np.random.default_rng(seed)
     return [round(float(g), 6) for g in rng.uniform(0.1, 1.0, 3)]
 
 
 def four_level(side=None, steps=8000, duration=400.0, full=2048):
+    """The four-level interferogram model of the module docstring (``side``: a strided subgrid
+    of the ``full`` x ``full`` grid)."""
     eps, A, Drive, t = sp.symbols("eps A Drive t", real=True)
     g = four_level_couplings(0)
     H = sp.diag(0, eps, 2 * eps + sp.Float(1.3), 3 * eps + sp.Float(0.7)) + Drive * sp.diag(0, 1, 2, 3)
@@ -82,6 +87,7 @@ def four_level(side=None, steps=8000, duration=400.0, full=2048):
 
 
 def duffing(side=None, full=1024, duration=500.0, intervals=512, seed=0):
+    """The driven Duffing oscillator of the module docstring as an ``odesolve_2D`` workload."""
     x, v, t, F, W = sp.symbols("x v t F W", real=True)
     rhs = [v, -0.1 * v - x - x**3 + F * sp.cos(W * t)]
     Fs = _axis(0.0, 2.0, full, side)
