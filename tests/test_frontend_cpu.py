@@ -89,3 +89,17 @@ def test_package_import_needs_no_cupy_or_triton():
             "assert not bad, bad\n") % str(pkg)
     proc = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
     assert proc.returncode == 0, proc.stderr[-2000:]
+
+
+def test_rabi_rhs_at_the_ground_state():
+    """After the reference's environment check (gqis/check_environment.py:284-293): for
+    H = (A/2) sigma_x at rho = |0><0|, d rho/dt = -i[H, rho] has Im(rho_01)' = A/2 and the rest 0."""
+    from gqis import compile_lindblad_rhs
+    A, dummy, Drive = sp.symbols("A dummy Drive", real=True)
+    rhs = compile_lindblad_rhs(Drive / 2 * sp.Matrix([[0, 1], [1, 0]]), A, [], sp.diag(0, 1), [A, dummy])
+    assert rhs.state_size == 3 and len(rhs.equations) == 3
+    at_ground = dict(zip(rhs.state_symbols, (1, 0, 0)))
+    drive = rhs.drive_map[Drive] if isinstance(rhs.drive_map, dict) else rhs.drive_map
+    values = [float(sp.sympify(e).subs(Drive, drive).subs({**at_ground, sp.Symbol("ParX", real=True): 2.0}))
+              for e in rhs.equations]
+    np.testing.assert_allclose(values, [0.0, 0.0, 1.0], atol=1e-12)
