@@ -58,9 +58,9 @@ int gqis_serve_cancel(gqis_server* server, int64_t request_id);
 /* Error text of a FAILED request (the module's message of the failing launch) into buf[len]. */
 int gqis_serve_request_error(gqis_server* server, int64_t request_id, char* buf, int64_t len);
 
-/* Cancel queued requests, wait for the chunks in flight, stop the server thread and free the
- * server's streams, events and counters. No other call on the handle may be in progress (in any
- * thread) or follow: the handle is invalid afterwards. */
+/* Cancel every request that has not ended (queued ones at once, running ones after their chunks
+ * in flight), stop the server thread and free the server's streams, events and counters. No other
+ * call on the handle may be in progress (in any thread) or follow: the handle is invalid afterwards. */
 int gqis_serve_close(gqis_server* server);
 
 const char* gqis_serve_last_error(void);
