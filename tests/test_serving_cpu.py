@@ -142,3 +142,16 @@ def test_small_requests_go_before_large_ones_but_waiting_counts():
         fb, fs = srv.submit_launch(big), srv.submit_launch(small)
         [f.result(5) for f in (first, fb, fs)]
     assert fs.admitted_at < fb.admitted_at  # the small request passed the big one queued before it
+
+
+def test_close_drains_queued_and_running_requests():
+    """close() returns once every request submitted before it has finished; none is dropped."""
+    be = FakeBackend(polls=4)
+    srv = SweepServer(backend=be, memory_budget=1 << 20, chunk_points=16)
+    futs = [srv.submit_launch(_launch(k)) for k in range(4)]
+    srv.close(timeout=10)
+    assert not srv._thread.is_alive()
+    assert all(f.done() and f.state == DONE for f in futs)
+    for k, f in enumerate(futs):
+        assert np.all(f.result(0)["result"] == k + 1j * k)
+    assert srv.stats["completed"] == 4
