@@ -38,6 +38,39 @@ def test_model_module_builds_loads_and_exports_every_declared_symbol():
     assert not any(s.startswith("_ZN") and "gqfixed" in s for s in exported)  # templates stay hidden
 
 
+def test_model_module_rejects_invalid_descriptors_before_any_cuda_call():
+    """The descriptor check of ``gqis_sweep_launch`` runs before any CUDA call, and a zero-point launch
+    returns before one too, so both are testable without a GPU."""
+    lib = ctypes.CDLL(str(_module_path()))
+    lib.gqis_last_error.restype = ctypes.c_char_p
+    launch = lib.gqis_sweep_launch
+    launch.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+
+    def desc(**kw):
+        d = abi.SweepDesc(abi_version=abi.ABI_VERSION, num_x=3, num_y=1, num_steps=10, warmup_steps=0,
+                          point_begin=0, point_count=0, dt=0.1, t_in=0.0)
+        for k, v in kw.items():
+            setattr(d, k, v)
+        return d
+
+    def rejects(d, text):
+        assert launch(ctypes.byref(d), None) == 1
+        assert text in lib.gqis_last_error(), lib.gqis_last_error()
+
+    assert launch(None, None) == 1 and b"descriptor is NULL" in lib.gqis_last_error()
+    assert lib.gqis_model_info_get(None) == 1
+    rejects(desc(abi_version=abi.ABI_VERSION + 1), b"ABI version")
+    rejects(desc(num_x=0), b"sweep axes must be non-empty")
+    rejects(desc(point_begin=2, point_count=2), b"outside the 3-point grid")
+    rejects(desc(num_steps=0), b"num_steps must be at least 1")
+    rejects(desc(warmup_steps=11), b"warmup_steps must lie in")
+    rejects(desc(warmup_steps=10), b"needs at least one step after warmup")
+    rejects(desc(dt=0.0), b"dt must be positive")
+    rejects(desc(dt=float("inf")), b"dt must be positive")
+    rejects(desc(point_count=3), b"par_x, par_y and results are required")
+    assert launch(ctypes.byref(desc()), None) == 0  # no points: nothing to launch
+
+
 def _struct_fields(text, name):
     import re
     body = text[text.index(f"typedef struct {name}"):text.index(f"}} {name};")]
