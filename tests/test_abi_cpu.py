@@ -71,6 +71,22 @@ def test_model_module_rejects_invalid_descriptors_before_any_cuda_call():
     assert launch(ctypes.byref(desc()), None) == 0  # no points: nothing to launch
 
 
+def test_adjoint_scratch_size_and_modules_without_an_adjoint():
+    """``gqis_adjoint_scratch_bytes`` is host arithmetic: (checkpoints + one interval of recomputed
+    states) x S x points x 8 bytes; a module built without an adjoint answers GQIS_ERR_UNSUPPORTED."""
+    lib = ctypes.CDLL(str(_module_path()))  # S = 3, no adjoint
+    lib.gqis_last_error.restype = ctypes.c_char_p
+    nbytes = ctypes.c_int64()
+    assert lib.gqis_adjoint_scratch_bytes(ctypes.c_int64(1000), 4000, 64, ctypes.byref(nbytes)) == 0
+    assert nbytes.value == (63 + 64) * 3 * 1000 * 8  # ceil(4000 / 64) = 63 checkpoints
+    assert lib.gqis_adjoint_scratch_bytes(ctypes.c_int64(1000), 4000, 0, ctypes.byref(nbytes)) == 1
+    assert lib.gqis_adjoint_scratch_bytes(ctypes.c_int64(-1), 4000, 64, ctypes.byref(nbytes)) == 1
+    assert lib.gqis_adjoint_scratch_bytes(ctypes.c_int64(1), 4000, 64, None) == 1
+    P, S = ctypes.c_int32(), ctypes.c_int32()
+    assert lib.gqis_adjoint_info(ctypes.byref(P), ctypes.byref(S)) == 3
+    assert lib.gqis_adjoint_launch(None, None) == 3 and b"without an adjoint" in lib.gqis_last_error()
+
+
 def _struct_fields(text, name):
     import re
     body = text[text.index(f"typedef struct {name}"):text.index(f"}} {name};")]
