@@ -473,3 +473,34 @@ def test_calibrated_trace_keeps_the_sample_times_of_the_given_grid():
     np.testing.assert_allclose(times, plain_times, rtol=1e-12)
     assert trace.shape == plain_trace.shape
     assert final.num_steps % 32 == 0 and final.trace_stride == 8 * final.num_steps // 32
+
+
+@pytest.mark.parametrize("name", ["rk4", "lserk4", "lserk4f", "dp5", "ab5", "anas5", "tsit5", "alshina6",
+                                  "dop853", "tsit5a", "dop853a"])
+def test_each_module_selects_only_its_own_integrator(name):
+    """After the reference's tests/test_cuda_solvers.py:21-32: the generated module names exactly one
+    integrator (its template and solver id), and carries a Butcher tableau only when that template
+    reads one, with the method's stage count."""
+    from gqis.cuda_solvers import get_solver_spec
+    x, t = sp.symbols("x t", real=True)
+    kw = {"solver_frequency": 1.0} if name == "anas5" else {}
+    with fake_device() as dev:
+        odesolve_2D([-x + sp.cos(t)], [x], [1.0], np.linspace(0.0, 1.0, 9), solver=name, fp64=True, **kw)
+    src = dev.sources[-1]
+    spec = get_solver_spec(name, frequency=1.0, step_size=0.125) if name == "anas5" else get_solver_spec(name)
+    solver_lines = [ln for ln in src.splitlines() if ln.startswith("#define GQ_SOLVER ")]
+    assert solver_lines == [f"#define GQ_SOLVER {spec.template}"]
+    assert f"#define GQ_SOLVER_ID {spec.solver_id}\n" in src
+    assert f"#define GQ_ADAPTIVE {1 if spec.adaptive else 0}\n" in src
+    if "gqmodel::Tableau" in spec.template:
+        assert src.count("struct Tableau {") == 1
+        assert f"static constexpr int NS = {len(spec.tableau.b)};" in src
+    else:
+        assert "struct Tableau" not in src
+
+
+def test_solver_ids_are_distinct():
+    from gqis.cuda_solvers import available_solvers, get_solver_spec
+    ids = [get_solver_spec(s, frequency=1.0, step_size=0.1).solver_id if s == "anas5" else get_solver_spec(s).solver_id
+           for s in available_solvers()]
+    assert len(set(ids)) == len(ids)
