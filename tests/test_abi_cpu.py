@@ -138,7 +138,12 @@ def test_solver_names_and_aliases():
 
 
 def test_solver_orders_rhs_counts_and_tableaus():
+    # steady-state RHS evaluations per step, FSAL reuse included (tests/test_cuda_solvers.py:35-42)
     assert get_solver_spec("rk4").rhs_evaluations == 4
+    assert get_solver_spec("lserk4").rhs_evaluations == 5
+    for name in ("dp5", "anas5", "tsit5"):
+        assert get_solver_spec(name, step_size=0.1).rhs_evaluations == 6
+    assert get_solver_spec("alshina6").rhs_evaluations == 7
     assert get_solver_spec("dop853").rhs_evaluations == 12
     assert get_solver_spec("ab5").rhs_evaluations == 1
     for name in ("dp5", "tsit5", "alshina6", "dop853"):
