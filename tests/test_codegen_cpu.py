@@ -504,3 +504,16 @@ def test_solver_ids_are_distinct():
     ids = [get_solver_spec(s, frequency=1.0, step_size=0.1).solver_id if s == "anas5" else get_solver_spec(s).solver_id
            for s in available_solvers()]
     assert len(set(ids)) == len(ids)
+
+
+def test_fitted_solver_parameter_is_a_runtime_value():
+    """After the reference's tests/test_cuda_solvers.py:56-59: anas5's frequency-fitted coefficient is
+    passed at launch, so other frequencies reuse the module."""
+    x, t = sp.symbols("x t", real=True)
+    with fake_device() as dev:
+        for f in (1.0, 1.14, 2.5):
+            odesolve_2D([-x + sp.cos(t)], [x], [1.0], np.linspace(0.0, 1.0, 9), solver="anas5", solver_frequency=f,
+                        fp64=True)
+    assert len(dev.sources) == 1
+    params = [launch.solver_params for launch in dev.launches]
+    assert all(len(p) == 1 for p in params) and len(set(params)) == 3
