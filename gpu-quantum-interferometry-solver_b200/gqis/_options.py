@@ -2,8 +2,9 @@
 
 The group table is part of the public interface of the reference package
 (``gqis/_options.py:7-18``): callers may pass e.g. ``codegen=dict(cse_batch_size=8)``
-instead of the flat keyword. The group names and their members are therefore kept
-identical; the merge logic below is this package's own.
+instead of the flat keyword, so the group names and members are the reference's, plus this
+engine's ``precision`` and ``rhs_form``. The error messages are the reference's too (its tests
+match them).
 """
 
 from collections.abc import Mapping
@@ -23,42 +24,47 @@ OPTION_GROUPS = {
 }
 
 
-def _still_default(value, default):
-    """True when ``value`` is the untouched signature default of a flat option."""
-    if value is default:
-        return True
-    simple = (bool, int, float, str, tuple)
-    return isinstance(default, simple) and type(value) is type(default) and value == default
+_PLAIN_DEFAULTS = (bool, int, float, str, tuple)
+
+
+def _untouched(value, default):
+    """A flat option counts as set by the caller unless it is its signature default (the object
+    itself, or an equal value of the same plain type)."""
+    return value is default or (isinstance(default, _PLAIN_DEFAULTS) and type(value) is type(default)
+                                and value == default)
+
+
+def _grouped(groups):
+    """``(group, option, value)`` for every option given inside a group, checked against the table."""
+    for group, given in groups.items():
+        if given is None:
+            continue
+        if not isinstance(given, Mapping):
+            raise TypeError(f"{group} must be a dict of option names and values.")
+        members = OPTION_GROUPS[group]
+        for option, value in given.items():
+            if option not in members:
+                raise ValueError(f"Unknown {group} option '{option}'. Valid options: {', '.join(members)}.")
+            yield group, option, value
 
 
 def apply_option_groups(func, args, groups, extra=None):
-    """Fold grouped options into the flat keyword dict ``args`` of ``func``.
+    """Move options given inside groups into the flat keyword dict ``args`` of ``func``.
 
-    ``groups`` maps a group name to a dict (or None); ``extra`` is the ``**option_set``
-    dict of a function that forwards unknown options. Each option may be given either
-    flat or inside its group; giving it both ways, naming an option that does not belong
-    to the group, or naming one that ``func`` cannot accept raises ``ValueError``
-    (behaviour of ``gqis/_options.py:30-57``).
+    ``groups`` maps a group name to a dict or None; ``extra`` is the ``**option_set`` dict of a
+    function that forwards options it does not name. An option goes to ``args`` when ``func``
+    names it, else to ``extra``; one given both flat and in its group, one outside its group, or
+    one that ``func`` cannot take raises ``ValueError``. Returns ``(args, extra)``.
     """
-    signature = inspect.signature(func).parameters
-    for group_name, members in groups.items():
-        if members is None:
-            continue
-        if not isinstance(members, Mapping):
-            raise TypeError(f"{group_name} must be a dict of option names and values.")
-        allowed = OPTION_GROUPS[group_name]
-        for name, value in members.items():
-            if name not in allowed:
-                raise ValueError(f"Unknown {group_name} option '{name}'. "
-                                 f"Valid options: {', '.join(allowed)}.")
-            if name in signature:
-                if not _still_default(args[name], signature[name].default):
-                    raise ValueError(f"'{name}' is given both directly and in {group_name}; use one.")
-                args[name] = value
-            elif extra is not None:
-                if name in extra:
-                    raise ValueError(f"'{name}' is given both directly and in {group_name}; use one.")
-                extra[name] = value
-            else:
-                raise ValueError(f"{func.__name__} does not accept the {group_name} option '{name}'.")
+    defaults = {name: p.default for name, p in inspect.signature(func).parameters.items()}
+    for group, option, value in _grouped(groups):
+        if option in defaults:
+            target, taken = args, not _untouched(args[option], defaults[option])
+        elif extra is not None:
+            target, taken = extra, option in extra
+        else:
+            raise ValueError(f"{func.__name__} does not accept the {group} option '{option}'.")
+        if taken:
+            raise ValueError(f"'{option}' is given both directly and in {group}; use one.")
+        target[option] = value
     return args, extra

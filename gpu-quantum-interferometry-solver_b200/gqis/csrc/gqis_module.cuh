@@ -30,6 +30,12 @@
 #ifndef GQ_ADJOINT_FINAL
 #define GQ_ADJOINT_FINAL 0  // adjoint of the final <O> instead of the time average
 #endif
+#ifndef GQ_PACK2
+#define GQ_PACK2 0  // FP32 RK4 with two points per thread in packed f32x2 arithmetic
+#endif
+#if GQ_PACK2
+#include "gqis_packed.cuh"
+#endif
 
 namespace {
 
@@ -71,6 +77,12 @@ static_assert(std::is_same<typename Model::real, typename Form::real>::value, "m
 constexpr auto kKernel = gqadaptive::sweep_adaptive_kernel<GQ_SOLVER, Model, Form, GQ_OUT, GQ_TRACE>;
 constexpr int kBlock = GQ_BLOCK;
 constexpr size_t kSmem = 0;
+#elif GQ_PACK2
+constexpr auto kKernel = gqpacked::sweep_pair_kernel<Model, GQ_OUT, GQ_TRACE>;
+constexpr int kBlock = GQ_BLOCK;
+constexpr size_t kSmem = 0;
+static_assert(Form::id == GQIS_FORM_FP32 && GQ_SOLVER_ID == GQIS_SOLVER_RK4,
+              "the packed two-point kernel is the FP32 form of RK4");
 #else
 constexpr auto kKernel = gqfixed::sweep_fixed_kernel<GQ_SOLVER, Model, Form, GQ_OUT, GQ_TRACE>;
 constexpr int kBlock = GQ_BLOCK;
@@ -109,6 +121,35 @@ int check_desc(const gqis_sweep_desc* d) {
 #endif
     return GQIS_OK;
 }
+
+#if GQ_ADAPTIVE
+// The persistent work-stealing launch shared by gqis_sweep_launch and gqis_sweep_launch_noalloc:
+// the grid is every resident CTA slot of the device, and lanes take point indices from the 32-bit
+// counter d.work_counter. Its range bounds a launch to GQIS_NOALLOC_MAX_POINTS points (2^31 - 1):
+// beyond that the counter would wrap and no lane would ever see the grid exhausted. The check
+// comes before any CUDA call.
+int launch_adaptive(const gqis_sweep_desc& d, cudaStream_t st) {
+    if (d.point_count > GQIS_NOALLOC_MAX_POINTS)
+        return fail(GQIS_ERR_TOO_LARGE, "adaptive launch: %lld points exceed the maximum of %lld per call",
+                    (long long)d.point_count, (long long)GQIS_NOALLOC_MAX_POINTS);
+    int dev = 0, sms = 0, ctas = 0;
+    cudaError_t e;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+        return cuda_fail(e, "cudaDeviceGetAttribute");
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas, kKernel, GQ_BLOCK, 0)) != cudaSuccess)
+        return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    if (ctas < 1) ctas = 1;
+    const int64_t needed = (d.point_count + GQ_BLOCK - 1) / GQ_BLOCK;
+    int64_t grid = GQ_STATIC_SCHEDULE ? needed : (int64_t)sms * ctas;
+    if (grid > needed) grid = needed;
+    if (grid > 0x7fffffffLL) return fail(GQIS_ERR_TOO_LARGE, "too many points for one launch");
+    kKernel<<<(unsigned)grid, GQ_BLOCK, 0, st>>>(d);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "adaptive sweep kernel launch");
+    return GQIS_OK;
+}
+#endif
 
 }  // namespace
 
@@ -175,27 +216,18 @@ __attribute__((visibility("default"))) int gqis_sweep_launch(const gqis_sweep_de
         kKernel<<<(unsigned)grid, kBlock, kSmem, st>>>(*d);
     }
 #elif GQ_ADAPTIVE
-    // Persistent grid: every resident CTA slot of the device, lanes refill themselves.
-    int dev = 0, sms = 0, ctas = 0;
-    cudaError_t e;
-    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
-    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
-        return cuda_fail(e, "cudaDeviceGetAttribute");
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas, kKernel, GQ_BLOCK, 0)) != cudaSuccess)
-        return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-    if (ctas < 1) ctas = 1;
-    const int64_t needed = (d->point_count + GQ_BLOCK - 1) / GQ_BLOCK;
-    int64_t grid = GQ_STATIC_SCHEDULE ? needed : (int64_t)sms * ctas;
-    if (grid > needed) grid = needed;
-    kKernel<<<(unsigned)grid, GQ_BLOCK, 0, st>>>(*d);
+    return launch_adaptive(*d, st);
 #else
-    const int64_t grid = (d->point_count + GQ_BLOCK - 1) / GQ_BLOCK;
+    const int64_t threads = GQ_PACK2 ? (d->point_count + 1) / 2 : d->point_count;  // packed: a pair per thread
+    const int64_t grid = (threads + GQ_BLOCK - 1) / GQ_BLOCK;
     if (grid > 0x7fffffffLL) return fail(GQIS_ERR_TOO_LARGE, "too many points for one launch");
     kKernel<<<(unsigned)grid, GQ_BLOCK, 0, st>>>(*d);
 #endif
+#if GQ_MATRIX || !GQ_ADAPTIVE
     cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) return cuda_fail(err, "sweep kernel launch");
     return GQIS_OK;
+#endif
 }
 
 }  // extern "C"
@@ -249,20 +281,7 @@ __attribute__((visibility("default"))) int gqis_sweep_launch_noalloc(const gqis_
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), st);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync(no-alloc work counter)");
-    int dev = 0, sms = 0, ctas = 0;
-    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
-    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
-        return cuda_fail(e, "cudaDeviceGetAttribute");
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas, kKernel, GQ_BLOCK, 0)) != cudaSuccess)
-        return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-    if (ctas < 1) ctas = 1;
-    const int64_t needed = (local.point_count + GQ_BLOCK - 1) / GQ_BLOCK;
-    int64_t grid = GQ_STATIC_SCHEDULE ? needed : (int64_t)sms * ctas;
-    if (grid > needed) grid = needed;
-    kKernel<<<(unsigned)grid, GQ_BLOCK, 0, st>>>(local);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_fail(e, "no-alloc sweep kernel launch");
-    return GQIS_OK;
+    return launch_adaptive(local, st);
 #else
     return gqis_sweep_launch(d, stream);  // fixed-step kernels use no scratch
 #endif

@@ -21,18 +21,16 @@ from __future__ import annotations
 import os
 import sys
 import time
-import warnings
 from contextlib import contextmanager
 from dataclasses import dataclass, field
 
 import numpy as np
-import sympy as sp
 
 from ._options import OPTION_GROUPS, apply_option_groups
-from .cuda_solvers import TSIT5A_DEFAULTS, counts_steps, get_solver_spec, normalize_solver_name
+from .cuda_solvers import counts_steps, get_solver_spec
 from .lindblad import build_independent_rho, build_reduced_lindblad_rhs, rho_matrix_to_independent_exprs
 from .rhs import _RHS_CODE_CACHE, CompiledRHS, compile_rhs as _compile_rhs_impl, runtime_const_values
-from . import emit
+from . import calibration, emit
 
 __all__ = ["mesolve_2D", "compile_lindblad_rhs", "CompiledRHS", "build_independent_rho",
            "build_reduced_lindblad_rhs", "rho_matrix_to_independent_exprs"]
@@ -40,22 +38,8 @@ __all__ = ["mesolve_2D", "compile_lindblad_rhs", "CompiledRHS", "build_independe
 _KERNEL_CACHE: dict = {}
 _TIMESTEP_CALIBRATION_CACHE: dict = {}
 
-TIMESTEP_CALIBRATION_DEFAULTS = {
-    "rms_atol": 1e-3, "rms_rtol": 0.0,
-    "max_atol": 1e-2, "max_rtol": 0.0,
-    "sample_stride": 8,
-    "max_steps": 2**20,
-    "min_step_tol": 1e-12,
-    "bisection_steps": 2,
-    "full_grid_bisection": False,
-    "recalibrate_every": None,
-    "reset": False,
-    "on_fail": "warning",
-    "range_warning": True,
-    "batch_levels": 1,
-}
-_CALIBRATION_MAX_HALVINGS = 6
-TIMESTEP_CALIBRATION_ODE_DEFAULTS = {"rms_atol": 1e-4, "max_atol": 1e-3}
+TIMESTEP_CALIBRATION_DEFAULTS = calibration.DEFAULTS
+TIMESTEP_CALIBRATION_ODE_DEFAULTS = calibration.ODE_DEFAULTS
 
 PRECISIONS = ("fp64", "fp32")
 MATRIX_FORM_FROM = 8  # rhs_form="auto" switches to the density-matrix kernels from this dimension
@@ -821,439 +805,29 @@ def _solve_symbolic_system(H, Drive, Col_Ops, mean_operator, tlist,
 
 
 # ----------------------------------------------------------------------------------------
-# calibrate_timesteps (gqis/solver.py:928-1341)
+# calibrate_timesteps (reference gqis/solver.py:928-1341): implemented in calibration.py. These
+# module-level names are the hooks the search calls through (and that tests replace).
 # ----------------------------------------------------------------------------------------
 
 def _timestep_calibration_settings(value, ode=False):
     """Validated ``calibrate_timesteps`` settings merged with the defaults."""
-    settings = dict(TIMESTEP_CALIBRATION_DEFAULTS)
-    if ode:
-        settings.update(TIMESTEP_CALIBRATION_ODE_DEFAULTS)
-    if value is not True:
-        if not isinstance(value, dict):
-            raise TypeError("calibrate_timesteps must be True, None or a dict of settings.")
-        unknown = set(value) - set(settings)
-        if unknown:
-            raise ValueError(f"Unknown calibrate_timesteps setting(s) {sorted(unknown)}. "
-                             f"Valid settings: {', '.join(settings)}.")
-        settings.update(value)
-    for name in ("rms_atol", "rms_rtol", "max_atol", "max_rtol"):
-        settings[name] = float(settings[name])
-        if settings[name] < 0.0:
-            raise ValueError(f"calibrate_timesteps {name} must be non-negative.")
-    settings["check_rms"] = settings["rms_atol"] > 0.0 or settings["rms_rtol"] > 0.0
-    settings["check_max"] = settings["max_atol"] > 0.0 or settings["max_rtol"] > 0.0
-    if not (settings["check_rms"] or settings["check_max"]):
-        raise ValueError("calibrate_timesteps needs at least one non-zero RMS or max tolerance.")
-    settings["sample_stride"] = int(settings["sample_stride"])
-    settings["max_steps"] = int(settings["max_steps"])
-    settings["min_step_tol"] = float(settings["min_step_tol"])
-    if settings["sample_stride"] < 1 or settings["max_steps"] < 1 or not settings["min_step_tol"] > 0.0:
-        raise ValueError("calibrate_timesteps sample_stride, max_steps and min_step_tol must be positive.")
-    settings["bisection_steps"] = int(settings["bisection_steps"])
-    if settings["bisection_steps"] < 0:
-        raise ValueError("calibrate_timesteps bisection_steps must be zero or a positive integer.")
-    settings["full_grid_bisection"] = bool(settings["full_grid_bisection"])
-    every = settings["recalibrate_every"]
-    if every is not None and int(every) < 1:
-        raise ValueError("calibrate_timesteps recalibrate_every must be None or a positive integer.")
-    settings["recalibrate_every"] = None if every is None else int(every)
-    if settings["on_fail"] not in {"warning", "ignore", "error"}:
-        raise ValueError("calibrate_timesteps on_fail must be 'warning', 'ignore' or 'error'.")
-    return settings
-
-
-def _is_adaptive(args):
-    return get_solver_spec(args["solver"]).adaptive
-
-
-def _timestep_calibration_key(args, settings):
-    """Model + accuracy request, independent of code-generation options."""
-    def key(e):
-        if isinstance(e, dict):
-            return frozenset((k, sp.sympify(v)) for k, v in e.items())
-        if isinstance(e, (list, tuple)):
-            return tuple(sp.sympify(x) for x in e)
-        if isinstance(e, sp.MatrixBase):
-            return e.shape, tuple(e)
-        return sp.sympify(e)
-
-    cv = args["const_values"] or {}
-    keep = args["keep_symbolic_consts"]
-    kept = set(args["runtime_consts"] or {})
-    if args["auto_runtime_consts"] or keep in ("all", "auto", "const_values"):
-        kept |= set(cv)
-    elif keep is not None:
-        kept |= set(keep)
-    fixed = tuple(sorted((str(k), float(v)) for k, v in cv.items() if k not in kept))
-    sweeps = tuple(str(s) for s in (args["var_arrays"] or {})) + tuple(
-        str(s) for s in (args["rho0_var_arrays"] or {}))
-    if args.get("compiled_rhs") is not None:
-        model = (args["compiled_rhs"].cache_key,)
-    else:
-        model = (key(args["H"]), key(args["Drive"]), tuple(key(L) for L in args["Col_Ops"]),
-                 key(args["mean_operator"]), key(args["rho0"]) if args["rho0"] is not None else None, fixed)
-    spec = get_solver_spec(args["solver"])
-    adaptive = None
-    if spec.adaptive:
-        opts = {**TSIT5A_DEFAULTS, **(args["adaptive_options"] or {})}
-        rtol, atol = float(opts["step_rtol"]), float(opts["step_atol"])
-        adaptive = (atol / rtol if rtol > 0.0 else np.inf, int(opts["max_substeps"]), settings["min_step_tol"])
-    return ("b200_timestep_calibration_v1", *model, sweeps, spec.name, adaptive, bool(args["fp64"]),
-            args.get("precision"), args["output_mode"], float(args["warmup_time"]), args["_ode_size"],
-            *(settings[n] for n in ("rms_atol", "rms_rtol", "max_atol", "max_rtol", "sample_stride",
-                                   "max_steps", "bisection_steps", "full_grid_bisection")))
-
-
-def _step_tolerance(args):
-    opts = {**TSIT5A_DEFAULTS, **(args["adaptive_options"] or {})}
-    return max(float(opts["step_rtol"]), float(opts["step_atol"]))
-
-
-def _scaled_adaptive_options(args, tol):
-    """adaptive_options with step_rtol and step_atol scaled together so the larger equals tol."""
-    opts = dict(args["adaptive_options"] or {})
-    merged = {**TSIT5A_DEFAULTS, **opts}
-    scale = tol / _step_tolerance(args)
-    opts.update(step_rtol=float(merged["step_rtol"]) * scale, step_atol=float(merged["step_atol"]) * scale)
-    return opts
-
-
-def _sweep_ranges(args):
-    out = []
-    for name in ("var_arrays", "rho0_var_arrays"):
-        for v in (args[name] or {}).values():
-            v = v if hasattr(v, "min") else np.asarray(v)
-            out.append((float(v.min()), float(v.max())))
-    return tuple(out)
+    return calibration.Settings.from_request(value, ode=ode)
 
 
 def _undersampled_arguments(args, stride):
-    """Arguments restricted to every stride-th point of each sweep axis (axis ends kept)."""
-    test = dict(args)
-    test.update(calibrate_timesteps=None, return_time_trace=False, return_timing_info=False, timings=False,
-                return_device=False, ignore_non_finite_output=True, Actual_Kernel_Save=False,
-                beep_on_error=False)
-
-    def picks(n):
-        idx = list(range(0, n, stride))
-        return idx if idx[-1] == n - 1 else idx + [n - 1]
-
-    def take(values, idx):
-        return [values[i] for i in idx] if isinstance(values, (list, tuple)) else values[idx]
-
-    axes, full = [], True
-    for name in ("var_arrays", "rho0_var_arrays"):
-        if args[name]:
-            test[name] = {}
-            for sym, values in args[name].items():
-                axes.append(picks(len(values)))
-                full = full and len(axes[-1]) == len(values)
-                test[name][sym] = take(values, axes[-1])
-    if args["rho0_values"] is not None:
-        v = args["rho0_values"]
-        v = v if hasattr(v, "ndim") else np.asarray(v)
-        v = v[axes[0]] if axes else v
-        test["rho0_values"] = v[:, axes[1]] if v.ndim == 3 and len(axes) > 1 else v
-    return test, full
+    """The call on every ``stride``-th point of each sweep axis (axis ends kept), and whether that
+    is the whole grid."""
+    return calibration.test_grid_arguments(args, stride)
 
 
 def _calibrate_timestep(args, settings, base_steps, duration):
-    """Coarsest resolution whose undersampled map meets the limits (``gqis/solver.py:1066-1216``).
-
-    Fixed-step solvers refine the step count by 2 (Richardson estimate with the method order,
-    order 1 for mean outputs); adaptive solvers refine 1/tolerance by 10 (error ~ tolerance).
-    A passing bracket is narrowed by ``bisection_steps`` geometric bisections.
-
-    Candidates of a fixed-step search are launched from one prepared launch of the test grid with
-    only the step count changed (no front-end pass per candidate). ``batch_levels`` > 1 runs the
-    next refinements (and later the next coarsenings) together, each candidate on its own stream with
-    one synchronisation; the candidates are then checked in the order of the one-at-a-time search, so
-    the outcome is the same. Speculative candidates beyond the accepted one cost device time.
-    """
-    start = time.time()
-    test, full_grid = _undersampled_arguments(args, settings["sample_stride"])
-    adaptive = _is_adaptive(args)
-    if adaptive:
-        factor, order = 10.0, 1
-        base, x_limit, label = 1.0 / _step_tolerance(args), 1.0 / settings["min_step_tol"], "step_tol"
-    else:
-        mean = args.get("output_mode") in ("mean", "mean_state") and float(args.get("warmup_time", 0.0)) < 1.0
-        factor, order = 2, (1 if mean else get_solver_spec(args["solver"]).order)
-        base, x_limit, label = base_steps, settings["max_steps"], "steps"
-
-    def value(x):
-        return 1.0 / x if adaptive else x
-
-    def coarser(x):
-        return x / factor if adaptive else x // 2
-
-    stored = {}
-    batch = max(1, int(settings.get("batch_levels", 1)))
-    results = {}
-    template = []  # a prepared launch of the test grid (fixed-step candidates differ only in steps)
-
-    def candidate(x):
-        t = dict(test)
-        if adaptive:
-            t["adaptive_options"] = _scaled_adaptive_options(args, value(x))
-        else:
-            t["tlist"] = np.linspace(0.0, duration, x + 1)
-        return t
-
-    def run_batch(xs):
-        xs = [x for x in dict.fromkeys(xs) if x not in results]
-        pending = []
-        for x in xs:
-            if template and not adaptive:  # only the step count differs: no front-end pass
-                pending.append((x, _with_steps(template[0], x, duration, args.get("warmup_time", 0.0))))
-                continue
-            holder = {}
-            ret = _solve_symbolic_system(**dict(candidate(x), _prepare_only=holder))
-            if "launch" in holder:
-                pending.append((x, holder["launch"]))
-                template.append(holder["launch"])
-            else:  # a solver stand-in that computes directly
-                results[x] = np.asarray(ret)
-        outs = _device_run_many([launch for _, launch in pending]) if pending else []
-        for (x, launch), out in zip(pending, outs):
-            results[x] = _calibration_map(launch, out[0])
-        if full_grid:
-            for x in xs:
-                stored[value(x)] = results[x]
-
-    def run(x):
-        run_batch([x])
-        return results[x]
-
-    def refinements(x):  # x refined `batch` times, as the search would step through them
-        out, c = [], x
-        for _ in range(batch):
-            c = factor * c
-            if c > x_limit:
-                break
-            out.append(c)
-        return out
-
-    def check(x, coarse, fine_x, fine):
-        rec = {label: value(x), "rms": np.inf, "max": np.inf}
-        if not (np.all(np.isfinite(coarse)) and np.all(np.isfinite(fine))):
-            return rec, False
-        scale = 1.0 / (1.0 - (x / fine_x) ** order)
-        diff = np.abs(fine - coarse) * scale
-        mag = np.abs(fine)
-        with np.errstate(over="ignore"):  # a diverging candidate's squares overflow to inf: rejected
-            rec.update(rms=float(np.sqrt(np.mean(diff**2))), max=float(np.max(diff)))
-            rms_lim = settings["rms_atol"] + settings["rms_rtol"] * float(np.sqrt(np.mean(mag**2)))
-        max_lim = settings["max_atol"] + settings["max_rtol"] * float(np.max(mag))
-        ok = ((not settings["check_rms"] or rec["rms"] <= rms_lim)
-              and (not settings["check_max"] or rec["max"] <= max_lim))
-        return rec, ok
-
-    run_batch([base] + refinements(base)[:batch - 1])
-    x, coarse = base, results[base]
-    tested, status, accepted = [], None, None
-    ref_x = ref = None
-    while status is None:
-        if factor * x > x_limit:
-            status, accepted = ("min_step_tol" if adaptive else "max_steps"), x
-            break
-        if factor * x not in results:
-            run_batch(refinements(x))
-        fine = results[factor * x]
-        if adaptive and np.all(np.isfinite(coarse)) and not np.all(np.isfinite(fine)):
-            status, accepted = "max_substeps", x
-            break
-        rec, ok = check(x, coarse, factor * x, fine)
-        tested.append(rec)
-        if ok:
-            status, accepted = "converged", x
-            ref_x, ref = factor * x, fine
-        elif len(tested) > 1 and np.isfinite(rec["rms"]) and rec["rms"] >= tested[-2]["rms"]:
-            best = min(tested, key=lambda r: r["rms"])
-            status, accepted = "precision_floor", (1.0 / best[label] if adaptive else best[label])
-        x, coarse = factor * x, fine
-
-    doubling = accepted
-    if status == "converged" and settings["bisection_steps"] > 0 and (settings["full_grid_bisection"] or not full_grid):
-        def passes(cand):
-            rec, ok = check(cand, run(cand), ref_x, ref)
-            tested.append({**rec, f"reference_{label}": value(ref_x)})
-            return ok
-
-        failing = coarser(accepted) if accepted > base else None
-        halvings = 0
-        while failing is None and (adaptive or accepted >= 2) and halvings < _CALIBRATION_MAX_HALVINGS:
-            halvings += 1
-            cand = coarser(accepted)
-            if cand not in results and batch > 1:  # the next coarsenings, as the loop would try them
-                seq, c = [], accepted
-                for _ in range(min(batch, _CALIBRATION_MAX_HALVINGS - halvings + 1)):
-                    if not (adaptive or c >= 2):
-                        break
-                    c = coarser(c)
-                    seq.append(c)
-                run_batch(seq)
-            if passes(cand):
-                accepted = cand
-            else:
-                failing = cand
-        for _ in range(settings["bisection_steps"] if failing is not None else 0):
-            cand = np.sqrt(failing * accepted)
-            cand = float(cand) if adaptive else int(round(cand))
-            if cand <= failing or cand >= accepted:
-                break
-            if passes(cand):
-                accepted = cand
-            else:
-                failing = cand
-
-    info = {"status": status, "tested": tested, "test_grid": coarse.shape[:2],
-            "calibration_s": time.time() - start, "full_grid_results": stored}
-    if adaptive:
-        info.update(step_tol=value(accepted), doubling_step_tol=value(doubling), start_step_tol=value(base))
-    else:
-        info.update(steps=accepted, dt=duration / accepted, doubling_steps=doubling)
-
-    def describe(x):
-        return f"step tolerance {value(x):.2e}" if adaptive else f"{x} steps"
-
-    if status != "converged":
-        def limit(kind):
-            atol, rtol = settings[f"{kind}_atol"], settings[f"{kind}_rtol"]
-            return f"{'RMS' if kind == 'rms' else 'max'} {atol:g}" + (f" + {rtol:g} relative" if rtol else "")
-        requested = ", ".join(limit(k) for k in ("rms", "max") if settings[f"check_{k}"])
-        reason = {"precision_floor": "does not converge",
-                  "max_steps": "is not reached within max_steps",
-                  "min_step_tol": "is not reached above min_step_tol",
-                  "max_substeps": ("needs more than max_substeps steps per output interval "
-                                   "(increase adaptive_options max_substeps)")}[status]
-        if tested:
-            best = next((r for r in tested if r[label] == value(accepted)), tested[-1])
-            achieved = (f"best achieved RMS {best['rms']:.2e}, max {best['max']:.2e} with {describe(accepted)}")
-        else:
-            achieved = f"no refinement beyond {describe(accepted)} was possible"
-        message = f"calibrate_timesteps: requested precision ({requested}) {reason}; {achieved}."
-        if status == "precision_floor" and not args["fp64"]:
-            message += " If better precision is required, consider switching to fp64=True."
-        if settings["on_fail"] == "error":
-            raise RuntimeError(message)
-        if settings["on_fail"] == "warning":
-            warnings.warn(message, RuntimeWarning, stacklevel=4)
-    return info
+    """Coarsest resolution whose undersampled map meets the limits (report dict)."""
+    return calibration.calibrate(args, settings, base_steps, duration)
 
 
 def _solve_with_timestep_calibration(args):
     """Pick a uniform step (or adaptive tolerance) on a subgrid, then run the full sweep."""
-    settings = _timestep_calibration_settings(args["calibrate_timesteps"], ode=args["_ode_size"] is not None)
-    tl = np.asarray(args["tlist"], dtype=np.float64)
-    if tl.ndim != 1 or len(tl) < 2:
-        raise ValueError("tlist must be a one-dimensional array with at least two samples.")
-    base_steps, duration = len(tl) - 1, float(tl[-1] - tl[0])
-    adaptive = _is_adaptive(args)
-    key = _timestep_calibration_key(args, settings)
-    entry = None if settings["reset"] else _TIMESTEP_CALIBRATION_CACHE.get(key)
-    calls = entry["calls"] if entry else 0
-    every = settings["recalibrate_every"]
-    ranges = _sweep_ranges(args)
-    info = None
-    if entry is None or (every is not None and calls % every == 0):
-        info = _calibrate_timestep(args, settings, base_steps, duration)
-        found = info["step_tol"] if adaptive else info["dt"]
-        stored = found if entry is None else min(entry["value"], found)
-        if entry is not None:
-            ranges = tuple((min(a[0], b[0]), max(a[1], b[1])) for a, b in zip(entry["ranges"], ranges))
-        entry = {"value": stored, "ranges": ranges, "range_warned": False}
-    else:
-        stored = entry["value"]
-        outside = any(lo < olo or hi > ohi for (lo, hi), (olo, ohi) in zip(ranges, entry["ranges"]))
-        if outside and settings["range_warning"] and not entry["range_warned"]:
-            entry["range_warned"] = True
-            warnings.warn("calibrate_timesteps: the sweep range extends beyond the range used for calibration; "
-                          "the stored step is reused without a new test. Use reset=True or recalibrate_every "
-                          "to test the new range.", RuntimeWarning, stacklevel=3)
-    entry["calls"] = calls + 1
-    _TIMESTEP_CALIBRATION_CACHE[key] = entry
-
-    run_args = dict(args, calibrate_timesteps=None)
-    if adaptive:
-        aligned, chosen = False, stored
-
-        def configure(tol):
-            run_args["adaptive_options"] = _scaled_adaptive_options(args, tol)
-        start_text = f"step tolerance {info['start_step_tol']:.2e}" if info else ""
-        chosen_text = f"step tolerance {chosen:.2e}"
-    else:
-        aligned = bool(args["return_time_trace"])
-        chosen = int(np.ceil(duration / stored * (1.0 - 1e-9)))
-        if settings["bisection_steps"] == 0 or aligned:
-            chosen = max(base_steps, chosen)
-        fac = 1
-        if aligned:
-            while base_steps * fac < chosen and base_steps * fac < settings["max_steps"]:
-                fac *= 2
-            chosen = base_steps * fac
-        chosen = min(chosen, max(base_steps, settings["max_steps"]))
-        if aligned and fac > 1:
-            if args["time_trace_samples_per_period"] is not None:
-                stride = max(1, int(round(int(args["solver_samples_per_period"])
-                                          / int(args["time_trace_samples_per_period"]))))
-            else:
-                stride = int(args["time_trace_every"] or 1)
-            run_args.update(time_trace_every=stride * fac, time_trace_samples_per_period=None,
-                            solver_samples_per_period=None, _time_trace_offset=fac - 1)
-
-        def configure(steps):
-            run_args["tlist"] = np.linspace(0.0, duration, steps + 1)
-        start_text = f"{base_steps} steps"
-        chosen_text = f"{chosen} steps"
-    configure(chosen)
-    if info is not None and args["timings"]:
-        last = (f"; last RMS/max change {info['tested'][-1]['rms']:.2e}/{info['tested'][-1]['max']:.2e}"
-                if info["tested"] else "")
-        print(f"calibrate_timesteps: {chosen_text} ({info['status']}), tested from {start_text} on "
-              f"{info['test_grid'][0]}x{info['test_grid'][1]} points in {info['calibration_s']:.2f}s{last}")
-
-    reusable = (info is not None and chosen in info["full_grid_results"] and not args["return_time_trace"]
-                and not args["return_timing_info"])
-    if reusable:
-        result = info["full_grid_results"][chosen]
-        if not np.all(np.isfinite(result)) and not args["ignore_non_finite_output"]:
-            raise RuntimeError("Non-finite values detected in mesolve_2D output. Try reducing dt "
-                               "(increase time samples) or check model parameters/RHS.")
-        if args["return_device"]:
-            import torch
-            return torch.as_tensor(result).cuda()
-        return result
-    finer = False
-    if info is not None:
-        doubling = info["doubling_step_tol"] if adaptive else info["doubling_steps"]
-        finer = doubling < chosen if adaptive else doubling > chosen
-    fallback = info is not None and info["status"] == "converged" and not aligned and finer
-    if fallback:
-        run_args["ignore_non_finite_output"] = True
-    result = _solve_symbolic_system(**run_args)
-    if fallback:
-        values = result[0] if isinstance(result, tuple) else result
-        if not _all_finite(values):
-            new_text = f"step tolerance {doubling:.2e}" if adaptive else f"{doubling} steps"
-            warnings.warn(f"calibrate_timesteps: {chosen_text} passed on the test points but gave non-finite "
-                          f"values on the full grid; using {new_text} instead.", RuntimeWarning, stacklevel=3)
-            chosen = doubling
-            entry["value"] = chosen if adaptive else duration / chosen
-            configure(chosen)
-            run_args["ignore_non_finite_output"] = args["ignore_non_finite_output"]
-            result = _solve_symbolic_system(**run_args)
-    if args["return_timing_info"]:
-        details = {k: v for k, v in info.items() if k != "full_grid_results"} if info else None
-        if adaptive:
-            opts = run_args["adaptive_options"]
-            report = {"step_tol": chosen, "step_rtol": opts["step_rtol"], "step_atol": opts["step_atol"]}
-        else:
-            report = {"steps": chosen, "dt": duration / chosen}
-        result[-1]["timestep_calibration"] = {**report, "calibrated_this_call": info is not None,
-                                              "details": details}
-    return result
+    return calibration.solve_calibrated(args)
 
 
 mesolve_2D.__doc__ = _solve_symbolic_system.__doc__

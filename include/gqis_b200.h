@@ -134,7 +134,9 @@ const char* gqis_last_error(void);
  *  - At most GQIS_NOALLOC_MAX_POINTS points per call (the counter's range); larger requests
  *    return GQIS_ERR_TOO_LARGE.
  *  - The first call on a device looks up the array's device address (once per device, with
- *    that device current); make that first call before any stream capture.
+ *    that device current); make that first call before any stream capture. The address is
+ *    kept per device ordinal for the life of the process: this entry point supports the
+ *    device's primary context only, and not a device reset (cudaDeviceReset) between calls.
  *  - Each call clears the counter on its stream before the kernel. All calls share the one
  *    array: calls whose kernels overlap on the GPU (other streams, other threads) race. */
 #define GQIS_NOALLOC_SCRATCH_BYTES 256

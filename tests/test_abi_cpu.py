@@ -71,6 +71,29 @@ def test_model_module_rejects_invalid_descriptors_before_any_cuda_call():
     assert launch(ctypes.byref(desc()), None) == 0  # no points: nothing to launch
 
 
+def test_adaptive_launch_rejects_more_points_than_its_work_counter_can_count():
+    """The adaptive kernels hand out points from a 32-bit counter, so one launch takes at most
+    2^31 - 1 points (a wrapped counter would never mark the grid exhausted). Both launches check
+    this before any CUDA call, so it is testable without a GPU."""
+    t, a, Drive = sp.symbols("t a Drive", real=True)
+    path = solver.prebuild("mesolve_2D", sp.Matrix([[a, Drive], [Drive, -a]]) / 2, sp.cos(t),
+                           [sp.Matrix([[0, 0.1], [0, 0]])], sp.diag(0, 1), np.linspace(0, 1, 11),
+                           var_arrays={a: np.linspace(-1, 1, 3)}, solver="tsit5a", fp64=True)
+    lib = ctypes.CDLL(str(path))
+    abi.bind_module(lib)
+    fake = 0x10000  # never dereferenced: the launch is refused first
+    d = abi.SweepDesc(abi_version=abi.ABI_VERSION, num_x=65536, num_y=65536, num_steps=10, warmup_steps=0,
+                      point_begin=0, point_count=1 << 32, dt=0.1, t_in=0.0, par_x=fake, par_y=fake,
+                      results=fake, work_counter=fake)
+    d.solver_params[0], d.solver_params[1], d.solver_params[2] = 1e-6, 1e-8, 64.0
+    for launch in (lib.gqis_sweep_launch, lib.gqis_sweep_launch_noalloc):
+        assert launch(ctypes.byref(d), None) == abi.ERR_TOO_LARGE
+        assert b"exceed the maximum" in lib.gqis_last_error()
+    d.point_count = (1 << 31) - 1  # at the limit the main launch passes the check and needs CUDA;
+    d.num_x = 0                    # an invalid axis makes it stop at the descriptor check instead
+    assert lib.gqis_sweep_launch(ctypes.byref(d), None) == abi.ERR_INVALID
+
+
 def test_adjoint_scratch_size_and_modules_without_an_adjoint():
     """``gqis_adjoint_scratch_bytes`` is host arithmetic: (checkpoints + one interval of recomputed
     states) x S x points x 8 bytes; a module built without an adjoint answers GQIS_ERR_UNSUPPORTED."""

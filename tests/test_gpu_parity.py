@@ -97,3 +97,34 @@ def test_adaptive_step_counts_match_reference():
     ref_acc = golden["adaptive_steps"][..., 0]
     assert np.mean(acc == ref_acc) >= 0.9
     assert np.max(np.abs(acc - ref_acc)) <= 2
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["c2_fp64_mean_sub32", "qubit_rk4_mean_warmup_trace", "qubit_rk4_final_rho"])
+def test_packed_pairs_match_the_one_point_kernel(name):
+    """Small FP32 RK4 models run two points per thread in packed f32x2 arithmetic. The map equals
+    the one-point-per-thread FP32 kernel's to FP32 rounding, and each point's result is bit for bit
+    the same whichever neighbour shares its thread (chunks that start at odd points, odd counts)."""
+    import torch
+    from pathlib import Path
+    from gqis import solver
+    case = CASES[name]
+    kw = dict(case["kwargs"], fp64=False)
+    packed = solver.prepare_sweep(case["api"], *case["args"], **kw)
+    assert "#define GQ_PACK2 1" in Path(str(packed.module.path).replace(".so", ".cu")).read_text()
+    single = solver.prepare_sweep(case["api"], *case["args"], **kw, nvrtc_options=("-DGQ_PACK2=0",))
+    packed.launch()
+    single.launch()
+    torch.cuda.synchronize()
+    a, b = packed.results.double().cpu().numpy(), single.results.double().cpu().numpy()
+    scale = max(1.0, float(np.max(np.abs(b))))
+    assert float(np.max(np.abs(a - b))) <= 1e-6 * scale
+    trace = packed.tensors.get("trace")
+    n = packed.points
+    for begin in (1, 7):
+        part = solver.prepare_sweep(case["api"], *case["args"], **kw, point_begin=begin, point_count=n - begin - 2)
+        part.launch()
+        torch.cuda.synchronize()
+        assert torch.equal(part.results, packed.results[begin:n - 2])
+        if trace is not None:
+            assert torch.equal(part.tensors["trace"], trace[begin:n - 2])
