@@ -126,7 +126,10 @@ def _barrier(ws):
         dist.barrier()
 
 
-def cpu_reference(steps=1, sample="c2_fp64_mean_sub64"):
+CPU_SAMPLE = "c2_fp64_mean_sub128"  # 128 x 128 strided subgrid of the 2048^2 grid, 8000 steps
+
+
+def cpu_reference(steps=1, sample=CPU_SAMPLE):
     """Reference kernel (GQIS-generated CUDA source compiled for the CPU) on host cores."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import ref_kernels
@@ -263,7 +266,8 @@ def run_ours(args):
     line = None
     if rank == 0:
         achieved = points * ksteps * flops_ps / (float(np.mean(t32)) / 1e3) / 1e12
-        traffic = _traffic_from_profiles().get("fp32_dram_bytes_per_launch")
+        measured = _traffic_from_profiles()
+        traffic = measured.get("fp32_dram_bytes_per_launch")
         lat = sorted(t32)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
@@ -278,7 +282,8 @@ def run_ours(args):
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peaks.get("fp32"), "unit": "TFLOP/s",
                          "frac": achieved / peaks["fp32"] if peaks.get("fp32") else None,
-                         "traffic": traffic, "peak_source": "measured FFMA probe (gqis_probe_fma) in this run",
+                         "traffic": traffic, "traffic_source": measured.get("fp32_traffic_source"),
+                         "peak_source": "measured FFMA probe (gqis_probe_fma) in this run",
                          "flops_per_point_step": flops_ps},
             "peaks_measured_tflops": peaks,
             "clocks": clocks,
@@ -287,11 +292,30 @@ def run_ours(args):
             "gpu_launches": args.steps,
         }
         if ws == 1 and not args.no_cpu_baseline:
-            ref = cpu_reference(steps=1, sample="c2_fp64_mean_sub128")
+            ref = cpu_reference(steps=1)
             line["cpu_baseline"] = {"value": ref["points"] * ref["steps"] / ref["times"][0], "unit": UNIT,
                                     "cores": ref["cores"], "kind": ref["kind"], "sample": ref["sample"]}
         if ws == 1 and args.reference_gpu and side == SIDE and nsteps == NSTEPS:
             line["reference_kernel_gpu"] = reference_gpu_kernels(ref_map)
+    if ws == 1 and not args.headline_only:
+        # the other configurations on the same GPU, after the headline measurement: C4 (Hilbert-space
+        # scaling on the tensor cores), C3 (adaptive Duffing) and C5 (serving)
+        del fp32, fp64
+        torch.cuda.empty_cache()
+        sys.path.insert(0, str(ROOT / "oracle"))
+        sampler = ClockSampler(local).start()
+        hpeaks = {"fp64": peaks["fp64"], "fp32": peaks["fp32"], "tf32_tensor": native.probe_tc_tf32_tflops()}
+        t_sub = time.perf_counter()
+        line["hilbert"] = {"workload": HILBERT_WORKLOAD.format(steps=2000), "l2": "flushed between timed launches",
+                           "measured_peaks_tflops": hpeaks,
+                           "per_dimension": hilbert_rows(torch, (8, 16, 32, 64), 2000, flush, hpeaks)}
+        line["duffing"] = {"workload": DUFFING_WORKLOAD.format(side=1024, solver="dop853a | tsit5a"),
+                           "per_solver": duffing_rows(torch, flush, 1024, 2, 1)}
+        del flush
+        torch.cuda.empty_cache()
+        line["serving"] = serving_summary(torch, args.sub_requests, args.rate, args.seed)
+        line["other_configs_wall_s"] = time.perf_counter() - t_sub
+        line["other_configs_clocks"] = sampler.stop()
     if ws > 1:
         import torch.distributed as dist
         dist.barrier()
@@ -321,71 +345,90 @@ def reference_gpu_kernels(fp64_map):
     return out
 
 
-def run_duffing(args):
-    """Config C3: adaptive sweep of the driven Duffing oscillator with a 512-sample state trace."""
+DUFFING_OPTIONS = {"step_rtol": 1e-8, "step_atol": 1e-10, "max_substeps": 2000, "count_steps": True}
+
+
+def duffing_rows(torch, flush, side, reps, warmup, solvers=("dop853a", "tsit5a"), reference_gpu=True,
+                 static_schedule=False):
+    """Config C3 per adaptive solver: the 1024^2 Duffing sweep (FP64, rtol 1e-8, atol 1e-10, final
+    state + 512-sample trace), accepted/rejected steps, and the final states on a 16 x 16 subgrid
+    against the C oracle of the same method and a tight-tolerance DOP853 reference; plus the
+    reference's own generated tsit5a kernel on the same GPU (final state, no trace)."""
     import numpy as np
-    import torch
-    torch.cuda.set_device(0)
-    sys.path.insert(0, str(ROOT / "oracle"))
-    from gqis import solver, workloads
-    side = args.side if args.side != SIDE else 1024
-    d = workloads.duffing(side=None, full=side)
-    opts = {"step_rtol": 1e-8, "step_atol": 1e-10, "max_substeps": 2000, "count_steps": True}
-    call = dict(var_arrays=d["var_arrays"], y0_values=d["y0_values"], solver=args.solver, fp64=True,
-                return_time_trace=True, adaptive_options=opts)
-    model = (d["rhs"], d["states"], None, d["tlist"])
-    sweep = solver.prepare_sweep("odesolve_2D", *model, **call)
-    flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
-    sampler = ClockSampler(0).start()
-    times = time_launches(torch, sweep, args.steps, args.warmup, flush)
-    clocks = sampler.stop()
-    counts = sweep.tensors["step_counts"].cpu().numpy().astype(np.int64)
-    acc, rej = int(counts[:, 0].sum()), int(counts[:, 1].sum())
-    ms = float(np.mean(times))
-    trace_bytes = sweep.tensors["trace"].numel() * sweep.tensors["trace"].element_size()
-    static = solver.prepare_sweep("odesolve_2D", *model, **call, nvrtc_options=("-DGQ_STATIC_SCHEDULE=1",))
-    static.launch()
-    torch.cuda.synchronize()
-    t_static = float(np.mean(time_launches(torch, static, 1, 0, flush)))
-    same = bool(torch.equal(static.results, sweep.results))
-    # accuracy on a 16 x 16 subgrid: the C oracle with the same method and tolerances, and a
-    # tight-tolerance DOP853 reference (points where the two oracle tolerances disagree by more than
-    # 1e-4 are flagged as chaotic and reported apart)
     import ode_oracle
+    from gqis import solver, workloads
+    d = workloads.duffing(side=None, full=side)
+    model = (d["rhs"], d["states"], None, d["tlist"])
     idx = np.round(np.linspace(0, side - 1, 16)).astype(int)
     F, W = (np.asarray(v)[idx] for v in d["var_arrays"].values())
     y0 = d["y0_values"][np.ix_(idx, idx)]
-    final = sweep.results.cpu().numpy().reshape(side, side, 2)[np.ix_(idx, idx)]
-    same_method, _, _ = ode_oracle.sweep(args.solver, F, W, y0, d["tlist"], rtol=1e-8, atol=1e-10,
-                                         max_substeps=2000, want_trace=False)
     tight, _, _ = ode_oracle.sweep("dop853a", F, W, y0, d["tlist"], rtol=1e-13, atol=1e-15,
                                    max_substeps=200000, want_trace=False)
     tight2, _, _ = ode_oracle.sweep("dop853a", F, W, y0, d["tlist"], rtol=1e-12, atol=1e-14,
                                     max_substeps=200000, want_trace=False)
-    chaotic = np.max(np.abs(tight - tight2), axis=-1) > 1e-4
-    err_same = np.max(np.abs(final - same_method), axis=-1)
-    err_true = np.max(np.abs(final - tight), axis=-1)
+    chaotic = np.max(np.abs(tight - tight2), axis=-1) > 1e-4  # points the tight references disagree on
+    rows = {}
+    for name in solvers:
+        call = dict(var_arrays=d["var_arrays"], y0_values=d["y0_values"], solver=name, fp64=True,
+                    return_time_trace=True, adaptive_options=DUFFING_OPTIONS)
+        sweep = solver.prepare_sweep("odesolve_2D", *model, **call)
+        ms = float(np.mean(time_launches(torch, sweep, reps, warmup, flush)))
+        counts = sweep.tensors["step_counts"].cpu().numpy().astype(np.int64)
+        acc, rej = int(counts[:, 0].sum()), int(counts[:, 1].sum())
+        trace_bytes = sweep.tensors["trace"].numel() * sweep.tensors["trace"].element_size()
+        final = sweep.results.cpu().numpy().reshape(side, side, 2)[np.ix_(idx, idx)]
+        same, _, _ = ode_oracle.sweep(name, F, W, y0, d["tlist"], rtol=1e-8, atol=1e-10, max_substeps=2000,
+                                      want_trace=False)
+        err_true = np.max(np.abs(final - tight), axis=-1)
+        row = {"ms": ms, "accepted_steps": acc, "rejected_steps": rej,
+               "points_accepted_steps_per_s": acc / (ms / 1e3),
+               "trace_bytes_per_launch": trace_bytes, "trace_write_gbs": trace_bytes / (ms / 1e3) / 1e9,
+               "subgrid_16x16_max_abs_vs_same_method_c_oracle": float(np.max(np.abs(final - same))),
+               "subgrid_16x16_max_abs_vs_tight_dop853_nonchaotic":
+                   float(err_true[~chaotic].max()) if (~chaotic).any() else None,
+               "chaotic_points_of_256": int(chaotic.sum())}
+        if static_schedule:
+            static = solver.prepare_sweep("odesolve_2D", *model, **call, nvrtc_options=("-DGQ_STATIC_SCHEDULE=1",))
+            row["static_schedule_ms"] = float(np.mean(time_launches(torch, static, 1, 1, flush)))
+            row["static_schedule_results_identical"] = bool(torch.equal(static.results, sweep.results))
+            row["work_stealing_speedup"] = row["static_schedule_ms"] / ms
+            del static
+        rows[name] = row
+        del sweep
+    if reference_gpu and "tsit5a" in solvers and side == 1024:
+        rows["reference_tsit5a_kernel_gpu"] = reference_tsit5a_gpu(torch, model, d, DUFFING_OPTIONS, flush)
+    return rows
+
+
+def run_duffing(args):
+    """Config C3: adaptive sweep of the driven Duffing oscillator with a 512-sample state trace."""
+    import torch
+    torch.cuda.set_device(0)
+    sys.path.insert(0, str(ROOT / "oracle"))
+    side = args.side if args.side != SIDE else 1024
+    flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    sampler = ClockSampler(0).start()
+    rows = duffing_rows(torch, flush, side, args.steps, args.warmup, solvers=(args.solver,),
+                        reference_gpu=args.reference_gpu, static_schedule=True)
+    clocks = sampler.stop()
+    row = rows[args.solver]
     line = {
         "metric": "points*accepted-steps/s (adaptive Duffing sweep, FP64, rtol 1e-8, atol 1e-10)",
-        "value": acc / (ms / 1e3), "unit": "points*accepted-steps/s", "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"driven Duffing x''+0.1x'+x+x^3=F cos(W t), {side}x{side} (F, W) grid, "
-                               f"t in [0, 500], {args.solver}, state trace 512 samples + final state",
+        "value": row["points_accepted_steps_per_s"], "unit": "points*accepted-steps/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": row["ms"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": DUFFING_WORKLOAD.format(side=side, solver=args.solver),
                    "l2": "flushed (256 MiB write) between timed launches"},
-        "accepted_steps": acc, "rejected_steps": rej, "points_intervals_per_s": side * side * 512 / (ms / 1e3),
-        "trace_bytes_per_launch": trace_bytes, "trace_write_gbs": trace_bytes / (ms / 1e3) / 1e9,
-        "static_schedule_ms": t_static, "work_stealing_speedup": t_static / ms,
-        "static_schedule_results_identical": same,
-        "subgrid_16x16": {"max_abs_vs_same_method_oracle": float(err_same.max()),
-                          "max_abs_vs_tight_dop853_nonchaotic": float(err_true[~chaotic].max()) if (~chaotic).any() else None,
-                          "chaotic_points": int(chaotic.sum())},
-        "clocks": clocks, "gpu_launches": args.steps,
+        **row, "clocks": clocks, "gpu_launches": args.steps,
     }
-    if args.reference_gpu and args.solver == "tsit5a" and side == 1024:
-        line["reference_kernel_gpu"] = reference_tsit5a_gpu(torch, model, d, opts, flush)
+    if "reference_tsit5a_kernel_gpu" in rows:
+        line["reference_kernel_gpu"] = rows["reference_tsit5a_kernel_gpu"]
     print(json.dumps(line))
     return 0
+
+
+DUFFING_WORKLOAD = ("driven Duffing x''+0.1x'+x+x^3=F cos(W t), {side}x{side} (F, W) grid, t in [0, 500], "
+                    "{solver}, state trace 512 samples + final state")
 
 
 def reference_tsit5a_gpu(torch, model, d, opts, flush):
@@ -459,89 +502,96 @@ def run_two_level(args):
     return 0
 
 
-def run_hilbert(args):
-    """Config C4: Hilbert-space scaling of the density-matrix kernel, N in {8, 16, 32, 64}, 64 x 64
-    (eps, A) points, 2000 RK4 steps on [0, 100]; FP64 and FP32 forms, error vs the FP64 oracle."""
+def hilbert_rows(torch, dims, hsteps, flush, peaks, *, tc_reps=3, fp64_reps=1, cuda_fp32=False):
+    """Config C4 per dimension N: the tensor-core FP32 form against the plain FP64 density-matrix
+    form on the full 64 x 64 map (both timed), the FP64 form pinned to the FP64 NumPy oracle on 4
+    points, and the tensor-core kernel's roofline by the algorithmic count (16 N^3 per product
+    pair, no split passes) and by the MMAs it issues (three split-TF32 passes)."""
     import numpy as np
-    import torch
-    torch.cuda.set_device(0)
-    sys.path.insert(0, str(ROOT / "oracle"))
     import lindblad_oracle
-    from gqis import native, solver, workloads
-    peaks = {"fp64": native.probe_fma_tflops(0), "fp32": native.probe_fma_tflops(1),
-             "tf32_tensor": native.probe_tc_tf32_tflops()}
-    dims = tuple(int(n) for n in args.dims.split(","))
-    flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    from gqis import solver, workloads
+    points = 64 * 64
     rows = {}
-    sampler = ClockSampler(0).start()
     for N in dims:
-        steps = args.hsteps
-        w = workloads.n_level(N, side=64, steps=steps, duration=100.0 * steps / 2000)
+        w = workloads.n_level(N, side=64, steps=hsteps, duration=100.0 * hsteps / 2000)
         model = (w["H"], w["Drive"], w["Col_Ops"], w["mean_operator"], w["tlist"])
-        points = 64 * 64
-        forms = [("matrix", "fp64"), ("matrix", "fp32")] + [("matrix_tc", "fp32")] + \
-                ([("reduced", "fp64"), ("reduced", "fp32")] if N <= 8 else [])
-        if args.forms:
-            forms = [f for f in forms if f"{f[0]}_{f[1]}" in args.forms.split(",")]
-        maps, row = {}, {}
-        for rhs_form, prec in forms:
+        forms = [("matrix_tc", "fp32", tc_reps, 1), ("matrix", "fp64", fp64_reps, 1 if N < 64 else 0)]
+        if cuda_fp32:
+            forms.append(("matrix", "fp32", tc_reps, 1))
+        row, maps = {}, {}
+        for rhs_form, prec, reps, warm in forms:
             sweep = solver.prepare_sweep("mesolve_2D", *model, var_arrays=w["var_arrays"], precision=prec,
                                          rhs_form=rhs_form)
-            reps = 1 if N >= 64 else max(1, args.steps // 2)
-            ms = float(np.mean(time_launches(torch, sweep, reps, 1, flush)))
-            flops = sweep.flops_per_point_step() * points * steps
-            rate = flops / (ms / 1e3) / 1e12
-            maps[(rhs_form, prec)] = sweep.results.double().cpu().numpy()
-            row[f"{rhs_form}_{prec}"] = {"ms": ms, "points_steps_per_s": points * steps / (ms / 1e3),
-                                         "flops_per_point_step": sweep.flops_per_point_step(),
-                                         "tflops": rate, "frac_of_measured_fma_peak": rate / peaks[prec]}
+            ms = float(np.mean(time_launches(torch, sweep, reps, warm, flush)))
+            frag = sweep.launch_spec.entry["frag"]
+            algo = frag["algorithmic_flops_per_point_step"] * points * hsteps / (ms / 1e3) / 1e12
+            entry = {"ms": ms, "points_steps_per_s": points * hsteps / (ms / 1e3), "timed_launches": reps,
+                     "warmup_launches": warm, "algorithmic_tflops": algo}
             if rhs_form == "matrix_tc":
-                tf = sweep.launch_spec.entry["frag"]["tensor_flops_per_point_step"] * points * steps
-                row[f"{rhs_form}_{prec}"]["tensor_pipe_tflops"] = tf / (ms / 1e3) / 1e12
-                row[f"{rhs_form}_{prec}"]["frac_of_measured_tf32_tensor_peak"] = tf / (ms / 1e3) / 1e12 / peaks["tf32_tensor"]
+                mma = frag["tensor_flops_per_point_step"] * points * hsteps / (ms / 1e3) / 1e12
+                entry.update(mma_tflops=mma, frac_mma_of_measured_tf32=mma / peaks["tf32_tensor"],
+                             frac_algorithmic_of_measured_tf32=algo / peaks["tf32_tensor"])
+            else:
+                entry["frac_algorithmic_of_measured_fma"] = algo / peaks[prec]
+            row[f"{rhs_form}_{prec}"] = entry
+            maps[(rhs_form, prec)] = sweep.results.double().cpu().numpy()
             del sweep
-        # the FP64 oracle on 4 points of the grid (full 2000 steps)
         eps, A = w["symbols"]
         idx = np.array([0, 21, 42, 63])
         sub = {eps: np.asarray(w["var_arrays"][eps])[idx[:2]], A: np.asarray(w["var_arrays"][A])[idx[2:]]}
         ref = lindblad_oracle.rk4_sweep(lindblad_oracle.from_workload(w, sub), w["tlist"]).reshape(-1)
         sel = (idx[:2][:, None] * 64 + idx[2:][None, :]).reshape(-1)
-        for key, m in maps.items():
+        full64 = maps[("matrix", "fp64")]
+        for (rhs_form, prec), m in maps.items():
             got = m[sel, 0] + 1j * m[sel, 1]
-            row[f"{key[0]}_{key[1]}"]["max_abs_err_vs_fp64_oracle_4pts"] = float(np.max(np.abs(got - ref)))
-        full64 = maps.get(("matrix", "fp64"))
-        if full64 is not None and ("matrix", "fp32") in maps:
-            row["matrix_fp32"]["max_abs_vs_matrix_fp64_full_map"] = float(np.max(np.abs(maps[("matrix", "fp32")] - full64)))
-            row["fp32_speedup_vs_fp64"] = row["matrix_fp64"]["ms"] / row["matrix_fp32"]["ms"]
-        if full64 is not None and ("matrix", "fp32") in maps and ("matrix_tc", "fp32") in maps:
-            row["matrix_tc_fp32"]["max_abs_vs_matrix_fp64_full_map"] = float(
-                np.max(np.abs(maps[("matrix_tc", "fp32")] - full64)))
-            row["tensor_core_speedup_vs_fp64"] = row["matrix_fp64"]["ms"] / row["matrix_tc_fp32"]["ms"]
-            row["tensor_core_speedup_vs_cuda_core_fp32"] = row["matrix_fp32"]["ms"] / row["matrix_tc_fp32"]["ms"]
-        rows[N] = row
+            row[f"{rhs_form}_{prec}"]["max_abs_vs_fp64_oracle_4pts"] = float(np.max(np.abs(got - ref)))
+            if prec == "fp32":
+                row[f"{rhs_form}_{prec}"]["max_abs_vs_fp64_form_full_map"] = float(np.max(np.abs(m - full64)))
+        row["tensor_core_speedup_vs_fp64"] = row["matrix_fp64"]["ms"] / row["matrix_tc_fp32"]["ms"]
+        rows[str(N)] = row
+    return rows
+
+
+def run_hilbert(args):
+    """Config C4: Hilbert-space scaling of the density-matrix kernel, N in {8, 16, 32, 64}, 64 x 64
+    (eps, A) points, 2000 RK4 steps on [0, 100]; FP64 and FP32 forms, error vs the FP64 oracle."""
+    import torch
+    torch.cuda.set_device(0)
+    sys.path.insert(0, str(ROOT / "oracle"))
+    from gqis import native
+    peaks = {"fp64": native.probe_fma_tflops(0), "fp32": native.probe_fma_tflops(1),
+             "tf32_tensor": native.probe_tc_tf32_tflops()}
+    dims = tuple(int(n) for n in args.dims.split(","))
+    flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    sampler = ClockSampler(0).start()
+    rows = hilbert_rows(torch, dims, args.hsteps, flush, peaks, tc_reps=max(1, args.steps // 2),
+                        cuda_fp32=True)
     clocks = sampler.stop()
-    head = rows[16 if 16 in rows else dims[0]]
-    hk = "matrix_tc_fp32" if "matrix_tc_fp32" in head else sorted(k for k in head if isinstance(head[k], dict))[0]
+    hk = "16" if "16" in rows else str(dims[0])
+    head = rows[hk]["matrix_tc_fp32"]
     line = {
         "metric": "points*steps/s (RK4 density-matrix sweep, N-level scaling model; tensor-core split-TF32 "
                   "form, N=16 headline)",
-        "value": head[hk]["points_steps_per_s"], "unit": "points*steps/s", "n_gpus": 1,
-        "steps": args.steps, "warmup": 1, "ms_per_step": head[hk]["ms"], "higher_is_better": True,
+        "value": head["points_steps_per_s"], "unit": "points*steps/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": 1, "ms_per_step": head["ms"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "N-level model: H0 seeded GUE-like + eps diag(0..N-1) + A cos(t) X; N-1 lowering "
-                               "ops at rate 0.01, N dephasing ops at rate 0.005; 64x64 (eps, A) grid, "
-                               f"{args.hsteps} RK4 steps of dt 0.05, mean <|N-1><N-1|>", "dims": list(dims),
+        "config": {"workload": HILBERT_WORKLOAD.format(steps=args.hsteps), "dims": list(dims),
                    "l2": "flushed (256 MiB write) between timed launches"},
-        "per_dimension": {str(k): v for k, v in rows.items()},
-        "roofline": ({"bound": "tensor", "achieved": head[hk]["tensor_pipe_tflops"], "peak": peaks["tf32_tensor"],
-                      "unit": "TFLOP/s", "frac": head[hk]["tensor_pipe_tflops"] / peaks["tf32_tensor"],
-                      "traffic": None, "peak_source": "tcgen05 kind::tf32 probe (gqis_probe_tc_tf32), same run",
-                      "kernel": f"matrix_tc_kernel N={16 if 16 in rows else dims[0]}"}
-                     if hk == "matrix_tc_fp32" else None),
+        "per_dimension": rows,
+        "roofline": {"bound": "tensor", "achieved": head["algorithmic_tflops"], "peak": peaks["tf32_tensor"],
+                     "unit": "TFLOP/s", "frac": head["frac_algorithmic_of_measured_tf32"], "traffic": None,
+                     "peak_source": "tcgen05 kind::tf32 probe (gqis_probe_tc_tf32), same run",
+                     "kernel": f"matrix_tc_kernel N={hk}", "mma_tflops": head["mma_tflops"],
+                     "frac_mma": head["frac_mma_of_measured_tf32"]},
         "measured_fma_peaks_tflops": peaks, "clocks": clocks,
     }
     print(json.dumps(line))
     return 0
+
+
+HILBERT_WORKLOAD = ("N-level model: H0 seeded GUE-like + eps diag(0..N-1) + A cos(t) X; N-1 lowering ops at rate "
+                    "0.01, N dephasing ops at rate 0.005; 64x64 (eps, A) grid, {steps} RK4 steps of dt 0.05, "
+                    "mean <|N-1><N-1|>")
 
 
 def run_render(args):
@@ -630,11 +680,10 @@ def run_fit(args):
     import numpy as np
     import torch
     torch.cuda.set_device(0)
-    sys.path.insert(0, str(ROOT / "tests"))
     sys.path.insert(0, str(ROOT / "oracle"))
     import gqis
     from gqis import adjoint, solver
-    from test_support_calls import qubit_fit_model
+    from gqis.workloads import qubit_fit_model
     fit_args, fit_kwargs, params = qubit_fit_model(side=(256, 256), steps=4000, duration=200.0)
     params = list(params[:3])
     prob = adjoint.Problem(*fit_args, **fit_kwargs, params=params)
@@ -691,28 +740,45 @@ def run_fit(args):
     return 0
 
 
-def run_serving(args):
-    """Config C5 (sweeps): Poisson stream of mixed-N, mixed-size sweep requests through the
-    continuous-batching server (FP32 form), against the same requests one by one on plain FP64."""
+def _central_difference_check(fit_args, fit_kwargs, params, grad, side=256, samples=16, h=1e-6):
+    """Max relative error of adjoint gradients against FP64 central differences on a strided subgrid."""
     import numpy as np
-    import torch
-    torch.cuda.set_device(0)
-    sys.path.insert(0, str(ROOT / "tests"))
-    sys.path.insert(0, str(ROOT / "oracle"))
+    import gqis
+    sel = np.round(np.linspace(0, side - 1, samples)).astype(int)
+    es, As = list(fit_kwargs["var_arrays"])
+    sub = dict(fit_kwargs, var_arrays={es: fit_kwargs["var_arrays"][es][sel], As: fit_kwargs["var_arrays"][As][sel]})
+    errs = []
+    for m, prm in enumerate(params):
+        up, dn = dict(sub["runtime_consts"]), dict(sub["runtime_consts"])
+        up[prm] += h
+        dn[prm] -= h
+        fd = (gqis.mesolve_2D(*fit_args, **dict(sub, runtime_consts=up), fp64=True).real
+              - gqis.mesolve_2D(*fit_args, **dict(sub, runtime_consts=dn), fp64=True).real) / (2 * h)
+        errs.append(float(np.max(np.abs(grad[np.ix_(sel, sel)][..., m] - fd)) / np.max(np.abs(fd))))
+    return errs
+
+
+SERVING_DIMS = (2, 4, 8, 16)
+
+
+def serving_summary(torch, requests, rate, seed, one_by_one=("fp32", "fp64"), fit_check=True):
+    """Config C5: a seeded Poisson stream of mixed-N, mixed-size sweep requests (FP32 form) and fit
+    requests (checkpointed FP64 adjoint) through the continuous-batching server; latency p50/p99
+    and aggregate points*steps/s, against the same requests run one by one through the public API
+    in the same form (what batching alone buys) and on the plain FP64 path."""
+    import numpy as np
     import gqis
     from gqis import adjoint
     from gqis.serving import SweepServer
-    from test_support_calls import SERVING_SIDES, qubit_fit_model, serving_model
-    rng = np.random.default_rng(args.seed)
-    dims = (2, 4, 8, 16)
-    reqs = []
-    t = 0.0
-    for _ in range(args.requests):
-        t += rng.exponential(1.0 / args.rate)
+    from gqis.workloads import SERVING_SIDES, qubit_fit_model, serving_model
+    rng = np.random.default_rng(seed)
+    reqs, t = [], 0.0
+    for _ in range(requests):
+        t += rng.exponential(1.0 / rate)
         if rng.random() < 0.2:
             reqs.append((t, "fit", 256))
         else:
-            N = int(rng.choice(dims))
+            N = int(rng.choice(SERVING_DIMS))
             sides = SERVING_SIDES if N < 16 else tuple(x for x in SERVING_SIDES if x <= 512)
             reqs.append((t, N, int(rng.choice(sides))))
     models = {}
@@ -721,10 +787,10 @@ def run_serving(args):
             models[(N, side)] = serving_model(N, side)
     fit_args, fit_kwargs, fit_params = qubit_fit_model(side=(256, 256), steps=4000, duration=200.0)
     fit_params = list(fit_params[:3])
-    for N in dims:  # warm the caches (symbolic model, module load) before timing
+    for N in SERVING_DIMS:  # warm the caches (symbolic model, module load) before timing
         a, kw = serving_model(N, 64)
-        gqis.mesolve_2D(*a, **kw, precision="fp32")
-        gqis.mesolve_2D(*a, **kw, precision="fp64")
+        for form in ("fp32",) + tuple(f for f in one_by_one if f != "fp32"):
+            gqis.mesolve_2D(*a, **kw, precision=form)
     adjoint.module_source(*fit_args, **fit_kwargs, params=fit_params)
 
     def steps_of(N, side):
@@ -747,50 +813,53 @@ def run_serving(args):
         stats = dict(srv.stats)
     lat = np.array([f.latency for f in futs]) * 1e3
     served = point_steps / (t_end - t0)
-    torch.cuda.synchronize()
-    t1 = time.perf_counter()
-    for _, N, side in reqs:  # the same requests one by one on the plain FP64 path
-        if N == "fit":
-            adjoint.mean_gradient(*fit_args, **fit_kwargs, params=fit_params)
-        else:
-            a, kw = models[(N, side)]
-            gqis.mesolve_2D(*a, **kw, precision="fp64")
-    torch.cuda.synchronize()
-    seq = point_steps / (time.perf_counter() - t1)
-    # one fit result against central differences (h = 1e-6, FP64) on a 16 x 16 strided subgrid
-    fit_check = None
+    baselines = {}
+    for form in one_by_one:  # the same requests one by one through the public API
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        for _, N, side in reqs:
+            if N == "fit":
+                adjoint.mean_gradient(*fit_args, **fit_kwargs, params=fit_params)
+            else:
+                a, kw = models[(N, side)]
+                gqis.mesolve_2D(*a, **kw, precision=form)
+        torch.cuda.synchronize()
+        rate_seq = point_steps / (time.perf_counter() - t1)
+        baselines[f"one_by_one_{form}"] = {"value": rate_seq, "served_speedup": served / rate_seq}
     fit_idx = [k for k, (_, N, _) in enumerate(reqs) if N == "fit"]
-    if fit_idx:
-        grad = outs[fit_idx[0]]["grad"]
-        sel = np.round(np.linspace(0, 255, 16)).astype(int)
-        (es, As) = list(fit_kwargs["var_arrays"])
-        sub = dict(fit_kwargs, var_arrays={es: fit_kwargs["var_arrays"][es][sel], As: fit_kwargs["var_arrays"][As][sel]})
-        errs = []
-        for m, p in enumerate(fit_params):
-            up, dn = dict(sub["runtime_consts"]), dict(sub["runtime_consts"])
-            up[p] += 1e-6
-            dn[p] -= 1e-6
-            fd = (gqis.mesolve_2D(*fit_args, **dict(sub, runtime_consts=up), fp64=True).real
-                  - gqis.mesolve_2D(*fit_args, **dict(sub, runtime_consts=dn), fp64=True).real) / 2e-6
-            g = grad[np.ix_(sel, sel)][..., m]
-            errs.append(float(np.max(np.abs(g - fd)) / np.max(np.abs(fd))))
-        fit_check = {"params": [str(p) for p in fit_params], "max_rel_err_vs_central_fd": errs}
+    check = None
+    if fit_check and fit_idx:
+        errs = _central_difference_check(fit_args, fit_kwargs, fit_params, outs[fit_idx[0]]["grad"])
+        check = {"params": [str(p) for p in fit_params], "max_rel_err_vs_central_fd": errs}
+    return {"value": served, "unit": "points*steps/s",
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                           "max": float(lat.max())},
+            **baselines, "requests": requests, "fit_requests": len(fit_idx), "total_point_steps": point_steps,
+            "workload": SERVING_WORKLOAD.format(requests=requests, rate=rate, dims=SERVING_DIMS, sides=SERVING_SIDES),
+            "server": "4 streams, 32768-point chunks, <= 16 admitted requests, memory budget 50% free",
+            "server_stats": stats, "fit_gradient_check": check}
+
+
+SERVING_WORKLOAD = ("{requests} seeded requests, Poisson rate {rate}/s; 80% sweeps (N uniform in {dims}, grid side "
+                    "uniform in {sides} (N = 16: up to 512), mean <O> maps, RK4, FP32 form; N = 8 and 16 on the "
+                    "tensor-core density-matrix kernel), 20% fits (d<O>avg/d(Gamma1, Gamma_phi, Delta), 256x256 "
+                    "two-level map, 4000 RK4 steps, checkpointed adjoint, FP64)")
+
+
+def run_serving(args):
+    """Config C5 (sweeps): Poisson stream of mixed-N, mixed-size sweep requests through the
+    continuous-batching server (FP32 form), against the same requests one by one."""
+    import torch
+    torch.cuda.set_device(0)
+    sys.path.insert(0, str(ROOT / "oracle"))
+    summary = serving_summary(torch, args.requests, args.rate, args.seed)
+    lat = summary["latency_ms"]
     line = {
         "metric": "sweep serving: aggregate points*steps/s and latency (Poisson 50/s, N in {2,4,8,16}, 20% fits)",
-        "value": served, "unit": "points*steps/s", "n_gpus": 1, "steps": args.requests, "warmup": len(dims),
-        "ms_per_step": float(np.mean(lat)), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"{args.requests} seeded requests, Poisson rate {args.rate}/s; 80% sweeps (N uniform "
-                               f"in {dims}, grid side uniform in {SERVING_SIDES} (N = 16: up to 512), mean <O> maps, RK4, "
-                               "FP32 form; N = 16 on the tensor-core density-matrix kernel), "
-                               "20% fits (d<O>avg/d(Gamma1, Gamma_phi, Delta), 256x256 two-level map, 4000 RK4 "
-                               "steps, checkpointed adjoint, FP64)",
-                   "server": "4 streams, 32768-point chunks, <= 16 admitted requests, memory budget 50% free"},
-        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
-                       "max": float(lat.max())},
-        "one_by_one_fp64": {"value": seq}, "speedup_vs_one_by_one_fp64": served / seq,
-        "server_stats": stats, "total_point_steps": point_steps, "fit_requests": len(fit_idx),
-        "fit_gradient_check": fit_check,
+        "value": summary["value"], "unit": "points*steps/s", "n_gpus": 1, "steps": args.requests,
+        "warmup": len(SERVING_DIMS), "ms_per_step": lat["p50"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": summary["workload"], "server": summary["server"]}, **summary,
     }
     print(json.dumps(line))
     return 0
@@ -808,6 +877,10 @@ def main():
     ap.add_argument("--reference-gpu", action="store_true",
                     help="also time the reference's generated kernels on this GPU")
     ap.add_argument("--requests", type=int, default=48, help="serving: number of requests")
+    ap.add_argument("--sub-requests", type=int, default=24,
+                    help="requests of the serving sub-object of the headline line")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="skip the C3/C4/C5 sub-objects of the headline line")
     ap.add_argument("--rate", type=float, default=50.0, help="serving: Poisson arrival rate (1/s)")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--dims", default="8,16,32,64", help="hilbert: Hilbert-space dimensions")

@@ -30,6 +30,8 @@ and zero population and stay exactly zero.
 
 from __future__ import annotations
 
+import os
+
 import hashlib
 from dataclasses import dataclass, field
 
@@ -279,10 +281,47 @@ def compile_matrix_model(H, Drive, Col_Ops, mean_operator, *, sweep_symbols, con
            None if model["rho0_exprs"] is None else tuple(sp.srepr(e) for e in model["rho0_exprs"]))
     if reuse and key in _CACHE:
         return _CACHE[key], "hit"
-    mm = decompose(model, sweep_symbols, key)
+    mm = _disk_load(key) if reuse else None
+    if mm is None:
+        mm = decompose(model, sweep_symbols, key)
+        if reuse:
+            _disk_store(key, mm)
     if reuse:
         _CACHE[key] = mm
     return mm, "miss"
+
+
+# Decomposing a dense model takes seconds (N = 64: ~18 s) and would repeat in every process;
+# decomposed models are pickled next to the model modules like prepared reduced-form RHS objects
+# (GQIS_DISK_CACHE=0 disables both).
+def _disk_load(key):
+    import pickle
+    from .rhs import _disk_path
+    if os.environ.get("GQIS_DISK_CACHE", "1") == "0":
+        return None
+    path = _disk_path(key)
+    try:
+        with open(path, "rb") as f:
+            stored_key, mm = pickle.load(f)
+    except Exception:
+        return None
+    return mm if stored_key == key else None
+
+
+def _disk_store(key, mm):
+    import pickle
+    from .rhs import _disk_path
+    if os.environ.get("GQIS_DISK_CACHE", "1") == "0":
+        return
+    path = _disk_path(key)
+    try:
+        path.parent.mkdir(parents=True, exist_ok=True)
+        tmp = path.with_suffix(f".{os.getpid()}.tmp")
+        with open(tmp, "wb") as f:
+            pickle.dump((key, mm), f, protocol=pickle.HIGHEST_PROTOCOL)
+        os.replace(tmp, path)
+    except Exception:
+        pass
 
 
 # ----------------------------------------------------------------------------------------
@@ -571,6 +610,20 @@ def flops_per_point_step(mm: MatrixModel):
     per_rhs = 8 * Np ** 3 + 4 * mm.num_dense * nn + (8 * nn + 4 * mm.num_diag * Np if mm.num_diag else 0)
     per_rhs += 2 * nn + 8 * nn + 8 * len(mm.jumps)
     return 4 * per_rhs + 26 * nn + 8 * nn
+
+
+def algorithmic_flops_per_point_step(mm: MatrixModel):
+    """Flops of one RK4 step of one point as the benchmark's roofline counts them, for any form:
+    per RHS the two complex N x N products of -i(H rho - rho H^dag) (16 N^3, 8 real flops per
+    complex multiply-add) plus the kernel's element-wise terms (coefficients, diagonal and jump
+    terms, -i(K - K^dag)); per step 4 RHS, the RK4 stage arithmetic (26 per element) and <O>
+    (8 per element). Uses the model's dimension N, not the padded tile, and counts neither the
+    padding nor the extra split-TF32 passes of the tensor-core kernel."""
+    N = mm.N
+    nn = N * N
+    elementwise = 4 * mm.num_dense * nn + (8 * nn + 4 * mm.num_diag * N if mm.num_diag else 0)
+    elementwise += 2 * nn + 8 * nn + 8 * len(mm.jumps)
+    return 4 * (16 * N ** 3 + elementwise) + 26 * nn + 8 * nn
 
 
 def tensor_flops_per_point_step(mm: MatrixModel):

@@ -627,7 +627,8 @@ def _solve_symbolic_system(H, Drive, Col_Ops, mean_operator, tlist,
                 "used_const_indices": tuple(range(len(const_vals))),
                 "flops_per_point_step": matrix_form.flops_per_point_step(compiled), "dimension": compiled.Np,
                 "tensor_cores": tensor_cores,
-                "tensor_flops_per_point_step": matrix_form.tensor_flops_per_point_step(compiled)}
+                "tensor_flops_per_point_step": matrix_form.tensor_flops_per_point_step(compiled),
+                "algorithmic_flops_per_point_step": matrix_form.algorithmic_flops_per_point_step(compiled)}
         stages["emit_s"] = 0.0
     elif RHSreuse and ekey in compiled.emitted:
         frag, stages["emit_s"] = compiled.emitted[ekey], 0.0

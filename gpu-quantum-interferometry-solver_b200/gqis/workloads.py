@@ -134,3 +134,38 @@ def n_level(N, side=64, steps=2000, duration=100.0, seed=0):
             "var_arrays": {eps: np.linspace(-0.5, 0.5, side), A: np.linspace(0.0, 2.0, side)},
             "const_values": {}, "symbols": (eps, A), "N": N, "H0": H0, "X": X, "D": D,
             "lowering_rate": 0.01, "dephasing_rate": 0.005, "omega": 1.0}
+
+
+# ---------------------------------------------------------------- serving and fit requests
+
+SERVING_SIDES = (64, 128, 256, 512, 1024)  # grid sides of the mixed serving stream (64^2 .. 1024^2)
+
+
+def serving_model(N, side):
+    """(args, kwargs) of one ``mesolve_2D`` serving request: the Lindblad model of dimension N
+    (two-level, four-level, or the N-level scaling model) on a side x side (eps, A) grid."""
+    if N == 2:
+        w = two_level()
+    elif N == 4:
+        w = four_level(full=side)
+    else:
+        w = n_level(N, side=side)
+    eps, A = w["symbols"]
+    var = {eps: np.linspace(float(np.min(w["var_arrays"][eps])), float(np.max(w["var_arrays"][eps])), side),
+           A: np.linspace(float(np.min(w["var_arrays"][A])), float(np.max(w["var_arrays"][A])), side)}
+    return ((w["H"], w["Drive"], w["Col_Ops"], w["mean_operator"], w["tlist"]),
+            {"var_arrays": var, "const_values": w["const_values"]})
+
+
+def qubit_fit_model(side=(8, 6), steps=400, duration=20.0):
+    """Fit-request model: the two-level qubit with Gamma1, Gamma_phi and Delta kept as runtime
+    constants (the parameters an interferogram fit adjusts; defaults 0.01, 0.02, 1.0) and drive
+    A cos(pi t). Returns (args, kwargs, (Gamma1, Gamma_phi, Delta, A))."""
+    eps, A, D, Drive, t, G1, Gp = sp.symbols("eps A Delta Drive t Gamma1 Gammaphi", real=True)
+    sz, sx, sm = sp.Matrix([[1, 0], [0, -1]]), sp.Matrix([[0, 1], [1, 0]]), sp.Matrix([[0, 1], [0, 0]])
+    H = eps / 2 * sz + D / 2 * sx + Drive * sz
+    args = (H, A * sp.cos(sp.pi * t), [sp.sqrt(G1) * sm, sp.sqrt(Gp / 2) * sz], sp.diag(0, 1),
+            np.linspace(0.0, duration, steps + 1))
+    kwargs = {"var_arrays": {eps: np.linspace(-3.0, 3.0, side[0]), A: np.linspace(0.0, 2.0, side[1])},
+              "runtime_consts": {G1: 0.01, Gp: 0.02, D: 1.0}}
+    return args, kwargs, (G1, Gp, D, A)

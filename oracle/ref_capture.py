@@ -35,7 +35,8 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
-DEFAULT_REFERENCE = Path("/root/reference")
+# the reference checkout beside this repository unless --reference or GQIS_REFERENCE_DIR names another
+DEFAULT_REFERENCE = Path(os.environ.get("GQIS_REFERENCE_DIR", str(HERE.parents[1] / "reference")))
 NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 OUTPUT_PARAMS = ("results", "time_trace_results", "adaptive_steps")
 

@@ -22,7 +22,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
-REFERENCE = Path(os.environ.get("GQIS_REFERENCE_DIR", "/root/reference"))
+REFERENCE = Path(os.environ.get("GQIS_REFERENCE_DIR", str(ROOT.parent / "reference")))
 OUT = ROOT / "oracle" / "_ref"
 
 

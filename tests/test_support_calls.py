@@ -21,23 +21,10 @@ def duffing_case(side=8, solver="dop853a", **extra):
     return d, (d["rhs"], d["states"], None, d["tlist"]), kwargs
 
 
-SERVING_SIDES = (64, 128, 256, 512, 1024)
-
-
-def serving_model(N, side):
-    """(args, kwargs) of one serving request: the Lindblad model of dimension N on a side^2 grid."""
-    W = ref_cases.workloads()
-    if N == 2:
-        w = W.two_level()
-    elif N == 4:
-        w = W.four_level(full=side)
-    else:
-        w = W.n_level(N, side=side)
-    eps, A = w["symbols"]
-    var = {eps: np.linspace(float(np.min(w["var_arrays"][eps])), float(np.max(w["var_arrays"][eps])), side),
-           A: np.linspace(float(np.min(w["var_arrays"][A])), float(np.max(w["var_arrays"][A])), side)}
-    return ((w["H"], w["Drive"], w["Col_Ops"], w["mean_operator"], w["tlist"]),
-            {"var_arrays": var, "const_values": w["const_values"]})
+# the serving and fit request models live with the other workloads (the serving bench uses them)
+SERVING_SIDES = ref_cases.workloads().SERVING_SIDES
+serving_model = ref_cases.workloads().serving_model
+qubit_fit_model = ref_cases.workloads().qubit_fit_model
 
 
 MATRIX_DIMS = (16, 32, 64)
@@ -121,17 +108,14 @@ def calls():
     return out
 
 
-def qubit_fit_model(side=(8, 6), steps=400, duration=20.0):
-    """Two-level model with Gamma1, Gamma_phi and Delta kept symbolic (fit parameters)."""
-    import sympy as sp
-    eps, A, D, Drive, t, G1, Gp = sp.symbols("eps A Delta Drive t Gamma1 Gammaphi", real=True)
-    sz, sx, sm = sp.Matrix([[1, 0], [0, -1]]), sp.Matrix([[0, 1], [1, 0]]), sp.Matrix([[0, 1], [0, 0]])
-    H = eps / 2 * sz + D / 2 * sx + Drive * sz
-    args = (H, A * sp.cos(sp.pi * t), [sp.sqrt(G1) * sm, sp.sqrt(Gp / 2) * sz], sp.diag(0, 1),
-            np.linspace(0.0, duration, steps + 1))
-    kwargs = {"var_arrays": {eps: np.linspace(-3.0, 3.0, side[0]), A: np.linspace(0.0, 2.0, side[1])},
-              "runtime_consts": {G1: 0.01, Gp: 0.02, D: 1.0}}
-    return args, kwargs, (G1, Gp, D, A)
+def config_calls():
+    """Module variants of the full-size configuration tests (tests/test_gpu_configs.py)."""
+    d = ref_cases.workloads().duffing(side=8)
+    base = dict(var_arrays=d["var_arrays"], y0_values=d["y0_values"], fp64=True,
+                adaptive_options={"step_rtol": 1e-8, "step_atol": 1e-10, "max_substeps": 2000})
+    args = (d["rhs"], d["states"], None, d["tlist"])
+    return [("odesolve_2D", args, dict(base, solver="tsit5a")),
+            ("odesolve_2D", args, dict(base, solver="dop853a", return_time_trace=True))]
 
 
 def adjoint_problems():

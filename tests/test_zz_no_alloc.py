@@ -49,6 +49,31 @@ def test_noalloc_launch_matches_the_allocating_launch_on_two_calls_in_a_row():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("name", ["qubit_rk4_final", "c2_fp64_mean_sub32"])
+def test_noalloc_launch_of_a_fixed_step_module_is_the_ordinary_launch(name):
+    """Fixed-step kernels use no scratch: the no-alloc entry point runs the ordinary launch and
+    ignores a NULL work counter (for the FP32 four-level case, the packed two-point kernel)."""
+    import torch
+    from gqis import abi, solver
+    torch.cuda.set_device(0)
+    case = ref_cases.cases()[name]
+    sweep = solver.prepare_sweep(case["api"], *case["args"], **dict(case["kwargs"], fp64=False))
+    stream = torch.cuda.current_stream()
+    sweep.launch(stream)
+    torch.cuda.synchronize()
+    expected = sweep.results.clone()
+    desc = abi.SweepDesc.from_buffer_copy(sweep.desc)
+    desc.work_counter = None
+    lib = sweep.module.lib
+    for call in range(2):
+        sweep.results.fill_(float("nan"))
+        rc = lib.gqis_sweep_launch_noalloc(ctypes.byref(desc), ctypes.c_void_p(stream.cuda_stream))
+        assert rc == abi.OK, lib.gqis_last_error().decode()
+        torch.cuda.synchronize()
+        assert torch.equal(sweep.results, expected), f"call {call}"
+
+
+@pytest.mark.gpu
 def test_noalloc_launch_rejects_more_points_than_its_scratch_can_count():
     import torch
     from gqis import abi, solver
