@@ -43,7 +43,10 @@ class AdjointDesc(ctypes.Structure):
                 ("scratch_bytes", ctypes.c_int64)]
 
 
+BATCH_MAX = 64  # GQIS_BATCH_MAX
+
 MODULE_SYMBOLS = ("gqis_model_info_get", "gqis_sweep_launch", "gqis_last_error", "gqis_sweep_launch_noalloc",
+                  "gqis_sweep_launch_batch",
                   "gqis_adjoint_info", "gqis_adjoint_scratch_bytes", "gqis_adjoint_launch")
 
 
@@ -55,6 +58,9 @@ def bind_module(lib):
     lib.gqis_sweep_launch.restype = ctypes.c_int
     lib.gqis_sweep_launch_noalloc.argtypes = [ctypes.POINTER(SweepDesc), ctypes.c_void_p]
     lib.gqis_sweep_launch_noalloc.restype = ctypes.c_int
+    lib.gqis_sweep_launch_batch.argtypes = [ctypes.POINTER(SweepDesc), ctypes.c_int32, ctypes.c_void_p,
+                                            ctypes.c_void_p]
+    lib.gqis_sweep_launch_batch.restype = ctypes.c_int
     lib.gqis_adjoint_info.argtypes = [ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]
     lib.gqis_adjoint_info.restype = ctypes.c_int
     lib.gqis_adjoint_scratch_bytes.argtypes = [ctypes.c_int64, ctypes.c_int32, ctypes.c_int32,

@@ -338,4 +338,55 @@ __global__ void __launch_bounds__(GQ_BLOCK, GQ_MIN_BLOCKS) sweep_adaptive_kernel
     }
 }
 
+// A batch: lanes take global point indices from the batch's one counter, so points of every item
+// share the persistent grid (a lane that finishes a point of one item may continue with a point of
+// another). Each lane keeps its item's descriptor; points are integrated exactly as in a launch of
+// their own.
+template <class Pair, class M, class F, int OUT, int TRACE>
+__global__ void __launch_bounds__(GQ_BLOCK, GQ_MIN_BLOCKS)
+    sweep_adaptive_batch_kernel(const __grid_constant__ BatchParams b) {
+    // lanes of a warp work on different items: their descriptors are read from shared memory
+    __shared__ gqis_sweep_desc items[GQIS_BATCH_MAX];
+    {
+        const int words = b.count * (int)(sizeof(gqis_sweep_desc) / sizeof(uint32_t));
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(b.items);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(items);
+        for (int w = threadIdx.x; w < words; w += blockDim.x) dst[w] = src[w];
+        __syncthreads();
+    }
+    const unsigned lane_id = threadIdx.x & 31u;
+    const int64_t total = b.starts[b.count];
+    Lane<Pair, M, F, OUT, TRACE> L;
+    const gqis_sweep_desc* dp = items;
+    double rtol = 0.0, atol = 0.0, inv_avg_time = 0.0;
+    int max_substeps = 0;
+    bool active = false, exhausted = false;
+    for (;;) {
+        const unsigned need = __ballot_sync(0xffffffffu, !active && !exhausted);
+        if (need) {
+            const int leader = __ffs(need) - 1;
+            unsigned base = 0;
+            if ((int)lane_id == leader) base = atomicAdd(b.counter, (unsigned)__popc(need));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (!active && !exhausted) {
+                const int64_t g = (int64_t)base + __popc(need & ((1u << lane_id) - 1u));
+                if (g < total) {
+                    const int i = batch_item(b, g);
+                    dp = items + i;
+                    rtol = dp->solver_params[0];
+                    atol = dp->solver_params[1];
+                    max_substeps = (int)dp->solver_params[2];
+                    inv_avg_time = 1.0 / ((double)(dp->num_steps - dp->warmup_steps) * dp->dt);
+                    L.start(*dp, g - b.starts[i]);
+                    active = true;
+                } else {
+                    exhausted = true;
+                }
+            }
+        }
+        if (!__any_sync(0xffffffffu, active)) break;
+        if (active && L.advance(*dp, rtol, atol, max_substeps, inv_avg_time)) active = false;
+    }
+}
+
 }  // namespace gqadaptive

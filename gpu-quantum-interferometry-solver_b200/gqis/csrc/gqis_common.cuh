@@ -174,6 +174,32 @@ struct FormFP32 {
 };
 
 // ---------------------------------------------------------------------------------------
+// Batches (gqis_sweep_launch_batch): up to GQIS_BATCH_MAX launches of one module in one grid.
+// The descriptors travel as the kernel's parameter (a __grid_constant__ struct of ~13 KB), so a
+// batch needs no device scratch and no copy. Item i owns the global work indices
+// [starts[i], starts[i + 1]) - threads of the fixed-step kernels (padded to whole warps, so that
+// a warp never mixes items), point pairs of the packed kernel (padded likewise), points of the
+// persistent adaptive kernels; starts[count] is the total.
+// ---------------------------------------------------------------------------------------
+struct BatchParams {
+    int32_t count;
+    uint32_t* counter;  // adaptive kernels: the batch's zeroed work-stealing counter
+    int64_t starts[GQIS_BATCH_MAX + 1];
+    gqis_sweep_desc items[GQIS_BATCH_MAX];
+};
+
+// The item whose range holds global index g (0 <= g < starts[count]): binary search.
+__device__ __forceinline__ int batch_item(const BatchParams& b, int64_t g) {
+    int lo = 0, hi = b.count;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (b.starts[mid] <= g) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// ---------------------------------------------------------------------------------------
 // Per-point context: sweep parameters, constants and static terms in FP64 (for drives) and
 // in the form's type (for the RHS and the observable).
 // ---------------------------------------------------------------------------------------

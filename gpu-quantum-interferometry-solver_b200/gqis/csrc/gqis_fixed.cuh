@@ -23,13 +23,15 @@ namespace gqfixed {
 // lanes. Not inlined: its FP64 transcendental code would otherwise raise the register count of
 // the whole integration loop; it runs once per kTimes/2 steps.
 template <class M, int kTimes>
-__device__ __noinline__ void fill_time_table(const gqis_sweep_desc& d, int step, int rank, int nlanes,
+// (dt and t_in are passed by value: a reference to the launch descriptor would force the kernels
+// to copy their descriptor parameter to local memory.)
+__device__ __noinline__ void fill_time_table(double dt, double t_in, int step, int rank, int nlanes,
                                              const double* Cd, double* tab) {
-    const double dt = d.dt, dt2d = dt * 0.5;
+    const double dt2d = dt * 0.5;
     for (int e = rank; e < kTimes; e += nlanes) {
         double te = ((double)(step + (e >> 1)) + 0.5) * dt;
         if (e & 1) te += dt2d;
-        M::time_funcs(d.t_in + te, Cd, tab + e * M::NTF);
+        M::time_funcs(t_in + te, Cd, tab + e * M::NTF);
     }
 }
 
@@ -73,7 +75,7 @@ struct RK4 {
             if constexpr (NTF > 0) {
                 if (slot == 0) {
                     __syncwarp(warp_mask);  // the previous chunk is consumed
-                    fill_time_table<M, kTimes>(d, step, rank, nlanes, pc.Cd, tab);
+                    fill_time_table<M, kTimes>(d.dt, d.t_in, step, rank, nlanes, pc.Cd, tab);
                     __syncwarp(warp_mask);
                 }
                 pc.drives_tf(d.t_in + t_mid, tab + (2 * slot) * NTF, Dr);
@@ -313,6 +315,21 @@ struct AdamsBashforth5 {
 template <class Solver, class M, class F, int OUT, int TRACE>
 __global__ void __launch_bounds__(GQ_BLOCK, GQ_MIN_BLOCKS) sweep_fixed_kernel(const gqis_sweep_desc d) {
     const int64_t local = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (local >= d.point_count) return;
+    Solver::template run<M, F, OUT, TRACE>(d, local, d.point_begin + local);
+}
+
+// A batch: item i covers threads [starts[i], starts[i + 1]), a whole number of warps (threads past
+// the item's points return), so each warp integrates points of one item and its time table serves
+// them all.
+template <class Solver, class M, class F, int OUT, int TRACE>
+__global__ void __launch_bounds__(GQ_BLOCK, GQ_MIN_BLOCKS)
+    sweep_fixed_batch_kernel(const __grid_constant__ BatchParams b) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= b.starts[b.count]) return;
+    const int i = batch_item(b, g);  // the same for the whole warp
+    const gqis_sweep_desc& d = b.items[i];
+    const int64_t local = g - b.starts[i];
     if (local >= d.point_count) return;
     Solver::template run<M, F, OUT, TRACE>(d, local, d.point_begin + local);
 }

@@ -54,7 +54,15 @@ namespace gqmatrix_tc {
 using gqmatrix::Cx;
 using gqmatrix::ldc;
 
-constexpr uint32_t kMaxPolls = 1u << 20;  // mbarrier polls before a wait gives up
+// mbarrier polls before an in-loop wait (MMA completion, partner's bytes) gives up. A build can
+// lower it (-DGQ_TC_MAX_POLLS=0 makes every such wait give up at once, which tests the give-up
+// path); the final wait for an MMA still in flight keeps the full limit, so no MMA writes tensor
+// memory after the kernel freed it.
+#ifndef GQ_TC_MAX_POLLS
+#define GQ_TC_MAX_POLLS (1u << 20)
+#endif
+constexpr uint32_t kMaxPolls = GQ_TC_MAX_POLLS;
+constexpr uint32_t kDrainPolls = 1u << 20;
 
 template <class MM>
 struct TcShape {
@@ -647,7 +655,7 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
     float* out = static_cast<float*>(d.results);
     if (failed) {
         // an MMA that did not signal: wait once more for it (bounded); mark the tile's outputs
-        if (mma_lost && tid == 0) gqtc::mbar_wait_bounded(bar, phase, kMaxPolls);
+        if (mma_lost && tid == 0) gqtc::mbar_wait_bounded(bar, phase, kDrainPolls);
         if (active && lead && crank == 0) {
             const int width = (OUT == GQIS_OUT_FINAL_STATE) ? MM::S : 2;
             for (int i = 0; i < width; ++i) out[(size_t)local * width + i] = __int_as_float(0x7fc00000);

@@ -12,6 +12,7 @@
 
 #include <stdarg.h>
 #include <stdio.h>
+#include <string.h>
 
 #include <mutex>
 
@@ -284,6 +285,97 @@ __attribute__((visibility("default"))) int gqis_sweep_launch_noalloc(const gqis_
     return launch_adaptive(local, st);
 #else
     return gqis_sweep_launch(d, stream);  // fixed-step kernels use no scratch
+#endif
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------
+// Batch launch (gqis_sweep_launch_batch): several sweeps of this module in one grid.
+// ---------------------------------------------------------------------------------------
+#if !GQ_MATRIX
+namespace {
+#if GQ_ADAPTIVE
+constexpr auto kBatchKernel = gqadaptive::sweep_adaptive_batch_kernel<GQ_SOLVER, Model, Form, GQ_OUT, GQ_TRACE>;
+#elif GQ_PACK2
+constexpr auto kBatchKernel = gqpacked::sweep_pair_batch_kernel<Model, GQ_OUT, GQ_TRACE>;
+#else
+constexpr auto kBatchKernel = gqfixed::sweep_fixed_batch_kernel<GQ_SOLVER, Model, Form, GQ_OUT, GQ_TRACE>;
+#endif
+
+// Global work units of one sweep in a batch: points (adaptive), or threads padded to whole warps
+// (one point, or one pair of points for the packed kernel, per thread).
+int64_t batch_units(const gqis_sweep_desc& d) {
+#if GQ_ADAPTIVE
+    return d.point_count;
+#elif GQ_PACK2
+    return ((d.point_count + 1) / 2 + 31) / 32 * 32;
+#else
+    return (d.point_count + 31) / 32 * 32;
+#endif
+}
+}  // namespace
+#endif
+
+extern "C" {
+
+__attribute__((visibility("default"))) int gqis_sweep_launch_batch(const gqis_sweep_desc* descs, int32_t count,
+                                                                    uint32_t* work_counter, void* stream) {
+#if GQ_MATRIX
+    (void)descs;
+    (void)count;
+    (void)work_counter;
+    (void)stream;
+    return fail(GQIS_ERR_UNSUPPORTED, "the density-matrix kernels have no batch launch");
+#else
+    if (!descs || count < 1) return fail(GQIS_ERR_INVALID, "batch: descs is NULL or count < 1");
+    if (count > GQIS_BATCH_MAX)
+        return fail(GQIS_ERR_TOO_LARGE, "batch of %d sweeps exceeds the maximum of %d", count, GQIS_BATCH_MAX);
+    static_assert(sizeof(BatchParams) <= 32000, "a batch must fit the kernel parameter space");
+    BatchParams b;
+    memset(&b, 0, sizeof(b));
+    b.count = count;
+    b.counter = work_counter;
+    int64_t total = 0;
+    for (int i = 0; i < count; ++i) {
+        b.items[i] = descs[i];
+#if GQ_ADAPTIVE
+        b.items[i].work_counter = work_counter;  // the batch's one counter
+#endif
+        const int rc = check_desc(&b.items[i]);
+        if (rc != GQIS_OK) {
+            char why[sizeof(g_last_error)];
+            snprintf(why, sizeof(why), "%s", g_last_error);
+            return fail(rc, "batch item %d: %s", i, why);
+        }
+        b.starts[i] = total;
+        total += batch_units(b.items[i]);
+    }
+    b.starts[count] = total;
+    if (total == 0) return GQIS_OK;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int64_t grid = (total + GQ_BLOCK - 1) / GQ_BLOCK;
+#if GQ_ADAPTIVE
+    if (total > GQIS_NOALLOC_MAX_POINTS)
+        return fail(GQIS_ERR_TOO_LARGE, "batch: %lld points exceed the maximum of %lld per launch", (long long)total,
+                    (long long)GQIS_NOALLOC_MAX_POINTS);
+    {
+        int dev = 0, sms = 0, ctas = 0;
+        cudaError_t e;
+        if ((e = cudaGetDevice(&dev)) != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+        if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+            return cuda_fail(e, "cudaDeviceGetAttribute");
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas, kBatchKernel, GQ_BLOCK, 0)) != cudaSuccess)
+            return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+        const int64_t resident = (int64_t)sms * (ctas < 1 ? 1 : ctas);
+        if (grid > resident) grid = resident;  // persistent: every resident CTA slot, lanes refill
+    }
+#endif
+    if (grid > 0x7fffffffLL) return fail(GQIS_ERR_TOO_LARGE, "too many points for one launch");
+    kBatchKernel<<<(unsigned)grid, GQ_BLOCK, 0, st>>>(b);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "batch sweep kernel launch");
+    return GQIS_OK;
 #endif
 }
 

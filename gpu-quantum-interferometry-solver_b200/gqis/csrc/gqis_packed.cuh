@@ -396,7 +396,7 @@ struct RK4x2 {
             if constexpr (NTF > 0) {
                 if (slot == 0) {
                     __syncwarp(warp_mask);
-                    gqfixed::fill_time_table<M, kTimes>(d, step, rank, nlanes, pc.Cd, tab);
+                    gqfixed::fill_time_table<M, kTimes>(d.dt, d.t_in, step, rank, nlanes, pc.Cd, tab);
                     __syncwarp(warp_mask);
                 }
                 pc.drives_tf(d.t_in + t_mid, tab + (2 * slot) * NTF, Dr);
@@ -443,6 +443,20 @@ struct RK4x2 {
 template <class M, int OUT, int TRACE>
 __global__ void __launch_bounds__(GQ_BLOCK, GQ_MIN_BLOCKS) sweep_pair_kernel(const gqis_sweep_desc d) {
     const int64_t pair = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t pair_count = (d.point_count + 1) / 2;
+    if (pair >= pair_count) return;
+    RK4x2::run<M, OUT, TRACE>(d, pair, pair_count);
+}
+
+// A batch: item i covers pairs [starts[i], starts[i + 1]), a whole number of warps of pairs.
+template <class M, int OUT, int TRACE>
+__global__ void __launch_bounds__(GQ_BLOCK, GQ_MIN_BLOCKS)
+    sweep_pair_batch_kernel(const __grid_constant__ BatchParams b) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= b.starts[b.count]) return;
+    const int i = batch_item(b, g);  // the same for the whole warp
+    const gqis_sweep_desc& d = b.items[i];
+    const int64_t pair = g - b.starts[i];
     const int64_t pair_count = (d.point_count + 1) / 2;
     if (pair >= pair_count) return;
     RK4x2::run<M, OUT, TRACE>(d, pair, pair_count);

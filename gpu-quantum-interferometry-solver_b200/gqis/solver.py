@@ -195,23 +195,38 @@ def _device_buffers(launch: SweepLaunch, point_begin=0, point_count=None):
 
 
 def _device_run_many(launches):
-    """Launch several sweeps at once, each on its own stream, and wait for all of them.
+    """Run several sweeps and wait for all of them; returns ``[(results, trace, step_counts, 0.0), ...]``.
 
-    Used by the batched calibration search: its candidate resolutions are small launches whose
-    results are only needed together. Returns ``[(results, trace, step_counts, 0.0), ...]``.
+    Used by the batched calibration search, whose candidate resolutions are small launches of one
+    module whose results are only needed together: sweeps of the same module go out as one
+    ``gqis_sweep_launch_batch`` grid (up to ``abi.BATCH_MAX`` per grid, one shared work counter for
+    the adaptive kernels). The density-matrix modules, which have no batch launch, get one launch
+    each on its own stream.
     """
+    from . import abi
     torch = _torch()
-    done = []
     current = torch.cuda.current_stream()
-    for launch in launches:
-        module = _load_kernel(launch.entry)
-        desc, buf = _device_buffers(launch)
-        stream = torch.cuda.Stream()
-        stream.wait_stream(current)  # inputs were uploaded on the current stream
-        module.launch(desc, stream.cuda_stream)
-        done.append(buf)
+    prepared = [(launch, _load_kernel(launch.entry), *_device_buffers(launch)) for launch in launches]
+    groups = {}
+    for k, (launch, module, desc, buf) in enumerate(prepared):
+        groups.setdefault(str(module.path), []).append(k)
+    for members in groups.values():
+        module = prepared[members[0]][1]
+        if prepared[members[0]][0].entry["frag"].get("matrix"):
+            for k in members:
+                stream = torch.cuda.Stream()
+                stream.wait_stream(current)  # inputs were uploaded on the current stream
+                module.launch(prepared[k][2], stream.cuda_stream)
+            continue
+        for start in range(0, len(members), abi.BATCH_MAX):
+            part = members[start:start + abi.BATCH_MAX]
+            descs = (abi.SweepDesc * len(part))(*[prepared[k][2] for k in part])
+            counter = torch.zeros(1, dtype=torch.int32, device=current.device)
+            rc = module.lib.gqis_sweep_launch_batch(descs, len(part), counter.data_ptr(), current.cuda_stream)
+            abi.check(rc, module.lib)
+            prepared[part[0]][3]["batch_counter"] = counter  # kept alive until the sync below
     torch.cuda.synchronize()
-    return [(b["results"], b["trace"], b["step_counts"], 0.0) for b in done]
+    return [(buf["results"], buf["trace"], buf["step_counts"], 0.0) for _, _, _, buf in prepared]
 
 
 def _with_steps(launch, steps, duration, warmup_time):

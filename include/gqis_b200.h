@@ -143,6 +143,22 @@ const char* gqis_last_error(void);
 #define GQIS_NOALLOC_MAX_POINTS 2147483647LL
 int gqis_sweep_launch_noalloc(const gqis_sweep_desc* desc, void* stream);
 
+/* No counterpart in the reference, which launches one sweep per kernel: up to GQIS_BATCH_MAX
+ * sweeps of this module (different grids, steps, dt, parameters and buffers; one model, solver,
+ * form and output mode) in ONE grid. Replaces a series of time_evolution_kernel launches
+ * (gqis/solver.py:2340), e.g. every candidate step count of one calibrate_timesteps search
+ * (gqis/solver.py:1131-1180) or point chunks of several serving requests.
+ *  - descs: a host array of count descriptors, each valid for gqis_sweep_launch; they travel as
+ *    the kernel's parameter, so the call needs no device scratch and makes no copy.
+ *  - Fixed-step modules: each sweep's points run as in a launch of their own.
+ *  - Adaptive modules: the points of all sweeps share one persistent grid and one work counter
+ *    (work_counter: one zeroed uint32 of device scratch; the descriptors' own counters are
+ *    ignored), so a lane that finishes a point of one sweep continues with any sweep's next
+ *    point; each point's result is the same as in a launch of its own.
+ *  - The density-matrix modules have no batch launch (GQIS_ERR_UNSUPPORTED). */
+#define GQIS_BATCH_MAX 64
+int gqis_sweep_launch_batch(const gqis_sweep_desc* descs, int32_t count, uint32_t* work_counter, void* stream);
+
 /* ---------------------------------------------------------------------------------------
  * Gradients (adjoint modules). No counterpart in the reference, which has no derivatives: a
  * module built with an adjoint (gqis.adjoint) also exports the functions below. For every point

@@ -226,3 +226,27 @@ def test_callers_template_directory_is_searched_before_the_packaged_headers(tmp_
     assert lib.gqis_test_override() == 7
     lib = ctypes.CDLL(str(engine.build_module(src)))
     assert lib.gqis_test_override() == 0
+
+
+def test_batch_launch_checks_its_arguments_before_any_cuda_call():
+    """``gqis_sweep_launch_batch`` validates the batch size and every descriptor on the host; a
+    density-matrix module answers GQIS_ERR_UNSUPPORTED."""
+    lib = ctypes.CDLL(str(_module_path()))
+    abi.bind_module(lib)
+    d = abi.SweepDesc(abi_version=abi.ABI_VERSION, num_x=3, num_y=1, num_steps=10, warmup_steps=0,
+                      point_begin=0, point_count=0, dt=0.1, t_in=0.0)
+    descs = (abi.SweepDesc * (abi.BATCH_MAX + 1))(*([d] * (abi.BATCH_MAX + 1)))
+    assert lib.gqis_sweep_launch_batch(descs, abi.BATCH_MAX + 1, None, None) == abi.ERR_TOO_LARGE
+    assert lib.gqis_sweep_launch_batch(descs, 0, None, None) == abi.ERR_INVALID
+    assert lib.gqis_sweep_launch_batch(None, 1, None, None) == abi.ERR_INVALID
+    descs[2].num_x = 0
+    assert lib.gqis_sweep_launch_batch(descs, 3, None, None) == abi.ERR_INVALID
+    assert b"batch item 2: sweep axes must be non-empty" in lib.gqis_last_error()
+    assert lib.gqis_sweep_launch_batch(descs, 2, None, None) == abi.OK  # no points: nothing to launch
+    from gqis import workloads
+    w = workloads.n_level(16, side=2, steps=10, duration=1.0)
+    path = solver.prebuild("mesolve_2D", w["H"], w["Drive"], w["Col_Ops"], w["mean_operator"], w["tlist"],
+                           var_arrays=w["var_arrays"], precision="fp64", rhs_form="matrix")
+    mlib = ctypes.CDLL(str(path))
+    abi.bind_module(mlib)
+    assert mlib.gqis_sweep_launch_batch(descs, 1, None, None) == abi.ERR_UNSUPPORTED

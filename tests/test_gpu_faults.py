@@ -37,3 +37,24 @@ def test_nan_parameter_poisons_only_its_points():
     out = gqis.mesolve_2D(*case["args"], **bad, ignore_non_finite_output=True)
     assert np.isnan(out[5].real).all()
     np.testing.assert_array_equal(np.delete(out, 5, axis=0), np.delete(clean, 5, axis=0))
+
+
+@pytest.mark.gpu
+def test_tensor_core_mma_wait_that_runs_out_marks_the_tile_nan_and_raises():
+    """The tensor-core kernel's waits for its MMAs are bounded. A build whose in-loop poll limit is 0
+    (no wait can succeed; the final wait for the MMA in flight keeps its full limit) takes the
+    give-up path on every tile: the CTA stops integrating, waits for the MMA it issued, writes NaN
+    for its points and frees its tensor memory. The call then raises like any non-finite map, and
+    the same process runs the ordinary kernel correctly afterwards."""
+    import gqis
+    from test_support_calls import GIVE_UP, hilbert_model
+    _, args, kwargs = hilbert_model(16)
+    common = dict(kwargs, precision="fp32", rhs_form="matrix_tc")
+    with pytest.raises(RuntimeError, match="Non-finite"):
+        gqis.mesolve_2D(*args, **common, nvrtc_options=GIVE_UP)
+    lost = gqis.mesolve_2D(*args, **common, nvrtc_options=GIVE_UP, ignore_non_finite_output=True)
+    assert np.isnan(np.asarray(lost).real).all()
+    good = gqis.mesolve_2D(*args, **common)
+    assert np.isfinite(good).all()
+    reference = gqis.mesolve_2D(*args, **dict(kwargs, precision="fp64", rhs_form="matrix"))
+    assert float(np.max(np.abs(good - reference))) <= 5e-6

@@ -68,3 +68,33 @@ def test_ode_front_end_known_answers():
     k = np.linspace(0.5, 2.0, 4)
     assert float(np.max(np.abs(out[:, 0] - np.exp(-2.0 * k)))) <= 1e-10
     assert float(np.max(np.abs(out[:, 1] - 2.0))) <= 1e-10
+
+
+@pytest.mark.gpu
+def test_tsit5a_matches_time_dependent_solution_between_coarse_output_points():
+    """Four output intervals on [0, 1.7]: the adaptive steps inside each interval follow the drive
+    (1 + 0.4 sin t) sx / 2, and rho00(T) = cos^2((T + 0.4 (1 - cos T)) / 2)
+    (the reference's tests/test_gpu_solver.py:271-290)."""
+    import gqis
+    from test_support_calls import tsit5a_coarse_output_call
+    args, kw = tsit5a_coarse_output_call()
+    rho = np.asarray(gqis.mesolve_2D(*args, **kw))
+    T = 1.7
+    expected = np.cos(0.5 * (T + 0.4 * (1.0 - np.cos(T)))) ** 2
+    assert abs(float(rho[0, 0, 0]) - expected) < 2.0e-7
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("fp64_time", (True, False))
+def test_tsit5a_time_average_integrates_over_adaptive_steps(fp64_time):
+    """The time average of rho00 = cos^2(t/2) over [2, 10] is 1/2 + (sin 10 - sin 2) / 16; Tsit5A
+    integrates it with the trapezoid rule over its own steps (second order, about
+    h^2/12 |f'(10) - f'(2)| / 8), not over the 5 output points (the reference's
+    tests/test_gpu_solver.py:294-311)."""
+    import gqis
+    from test_support_calls import tsit5a_average_call
+    args, kw = tsit5a_average_call(fp64_time)
+    value, info = gqis.mesolve_2D(*args, **kw)
+    expected = 0.5 + (np.sin(10.0) - np.sin(2.0)) / (2.0 * 8.0)
+    assert abs(float(np.real(value[0, 0])) - expected) < 5.0e-5
+    assert info["adaptive_steps"]["accepted"][0, 0] > 5

@@ -28,6 +28,7 @@ qubit_fit_model = ref_cases.workloads().qubit_fit_model
 
 
 MATRIX_DIMS = (16, 32, 64)
+GIVE_UP = ("-DGQ_TC_MAX_POLLS=0",)  # every in-loop MMA wait of the tensor-core kernel gives up at once
 TENSOR_DIMS = (8, 16, 32, 64)
 
 
@@ -53,6 +54,8 @@ def matrix_calls():
     for N in (16, 64):
         _, args, kwargs = hilbert_model(N)
         out.append(("mesolve_2D", args, dict(kwargs, precision="fp32", rhs_form="matrix_tc", output_mode="final_rho")))
+    _, args, kwargs = hilbert_model(16)  # the give-up path of the tensor-core kernel's MMA waits
+    out.append(("mesolve_2D", args, dict(kwargs, precision="fp32", rhs_form="matrix_tc", nvrtc_options=GIVE_UP)))
     _, args, kwargs = hilbert_model(64)  # the two-CTA tensor-core kernel's trace against the FP64 matrix form
     trace64 = dict(kwargs, return_time_trace=True, time_trace_every=9)
     out.append(("mesolve_2D", args, dict(trace64, fp64=True, rhs_form="matrix")))
@@ -116,6 +119,76 @@ def config_calls():
     args = (d["rhs"], d["states"], None, d["tlist"])
     return [("odesolve_2D", args, dict(base, solver="tsit5a")),
             ("odesolve_2D", args, dict(base, solver="dop853a", return_time_trace=True))]
+
+
+# driven dissipative qubit of the reference's calibration tests (tests/test_gpu_solver.py:131-227)
+CAL_W = 1.14
+CAL_PERIOD = 2.0 * np.pi / CAL_W
+
+
+def calibration_qubit_call(steps_per_period, periods=10, side=16, span=6.0, **options):
+    """(args, kwargs) of the driven qubit: H = Delta/2 sx + Drive/2 sz, Drive = eps + A sin(w t),
+    w = 1.14, L = sqrt(g1) s-, sqrt(g2) sz (g1 = 0.05 / period, g2 = g1 / 2 + 0.04 / period),
+    O = |1><1|; eps in +-span w, A in [0, span w] on a side x side grid."""
+    D, eps, Drive, A, t = sp.symbols("Delta eps Drive A t", real=True)
+    sz, sm, sx = sp.Matrix([[1, 0], [0, -1]]), sp.Matrix([[0, 1], [0, 0]]), sp.Matrix([[0, 1], [1, 0]])
+    g1 = 0.05 / CAL_PERIOD
+    g2 = g1 / 2.0 + 0.04 / CAL_PERIOD
+    axes = {eps: np.linspace(-span * CAL_W, span * CAL_W, side), A: np.linspace(0.0, span * CAL_W, side)}
+    args = (0.5 * D * sx + 0.5 * Drive * sz, eps + A * sp.sin(CAL_W * t), [sp.sqrt(g1) * sm, sp.sqrt(g2) * sz],
+            sp.diag(0, 1), np.linspace(0.0, periods * CAL_PERIOD, periods * steps_per_period + 1))
+    return args, dict(var_arrays=axes, const_values={D: 1.0}, **options)
+
+
+def calibration_oscillator_call(steps, **options):
+    """(args, kwargs) of the damped driven oscillator x'' = -d x' - x - 0.2 x^3 + a cos(1.3 t) of the
+    reference's ODE calibration test (tests/test_gpu_solver.py:234-266), 16 x 16 (d, a) grid."""
+    x, v, t, damping, amplitude = sp.symbols("x v t damping amplitude", real=True)
+    axes = {damping: np.linspace(0.1, 0.5, 16), amplitude: np.linspace(0.1, 1.0, 16)}
+    args = ([v, -damping * v - x - 0.2 * x**3 + amplitude * sp.cos(1.3 * t)], [x, v], [1.0, 0.0],
+            np.linspace(0.0, 20.0, steps + 1))
+    options = dict(options)
+    if options.pop("observable", False):
+        options["observable"] = x**2 + v**2
+    return args, dict(var_arrays=axes, **options)
+
+
+def calibration_calls():
+    """Module variants of the calibration and Tsit5A known-answer tests."""
+    out = []
+    for solver in ("rk4", "tsit5a"):
+        for mode in ("mean", "final", "final_rho"):
+            out.append(("mesolve_2D",) + calibration_qubit_call(8, output_mode=mode, solver=solver))
+        out.append(("mesolve_2D",) + calibration_qubit_call(8, output_mode="final", solver=solver,
+                                                            return_time_trace=True, time_trace_every=8))
+        for extra in ({}, {"output_mode": "mean"}, {"observable": True},
+                      {"return_time_trace": True, "time_trace_every": 8}):
+            out.append(("odesolve_2D",) + calibration_oscillator_call(64, solver=solver, **extra))
+    out.append(("mesolve_2D",) + tsit5a_coarse_output_call())
+    out.append(("mesolve_2D",) + tsit5a_average_call())
+    return out
+
+
+def tsit5a_coarse_output_call():
+    """H = (1 + (2/5) sin t) sx / 2 from |0>, 4 output intervals on [0, 1.7], Tsit5A at 1e-12
+    (tests/test_gpu_solver.py:271-290): rho00(T) = cos^2((T + 0.4 (1 - cos T)) / 2)."""
+    dummy, Drive, t = sp.symbols("dummy Drive t", real=True)
+    H = (1 + Drive) * sp.Matrix([[0, 1], [1, 0]]) / 2
+    kw = dict(var_arrays={dummy: np.array([0.0])}, output_mode="final_rho", solver="tsit5a", fp64=True,
+              adaptive_options={"step_rtol": 1e-12, "step_atol": 1e-12, "max_substeps": 10000})
+    return (H, {Drive: sp.Rational(2, 5) * sp.sin(t)}, [], sp.eye(2), np.linspace(0.0, 1.7, 5)), kw
+
+
+def tsit5a_average_call(fp64_time=True):
+    """H = sx / 2 from |0>, mean of |0><0| over [2, 10] (warmup 0.2 of 5 intervals of length 2),
+    Tsit5A at 1e-10 (tests/test_gpu_solver.py:294-311): 1/2 + (sin 10 - sin 2) / 16."""
+    dummy = sp.Symbol("dummy", real=True)
+    kw = dict(var_arrays={dummy: np.array([0.0])}, rho0=sp.Matrix([[1, 0], [0, 0]]), output_mode="mean",
+              warmup_time=0.2, solver="tsit5a", fp64=True, return_timing_info=True,
+              adaptive_options={"step_rtol": 1e-10, "step_atol": 1e-10, "fp64_time": fp64_time,
+                                "count_steps": True, "max_substeps": 10000})
+    return (sp.Matrix([[0, 1], [1, 0]]) / 2, sp.Integer(0), [], sp.Matrix([[1, 0], [0, 0]]),
+            np.linspace(0.0, 10.0, 6)), kw
 
 
 def adjoint_problems():
