@@ -140,10 +140,19 @@ def _positive_copy(expr):
     return expr.xreplace({s: sp.Symbol(str(s), positive=True) for s in expr.free_symbols})
 
 
-def decompose(model, sweep_symbols, cache_key):
-    """:class:`MatrixModel` of a model prepared by :func:`gqis.rhs.prepare_model`."""
-    N = int(model["N"])
+def tile_dimension(N, tensor_cores=False):
+    """Padded dimension of the kernel tile: :func:`padded_dimension`, except that a tensor-core
+    sweep of a model of dimension 33 .. 48 pads to 64 (the tcgen05 kernel takes 8, 16, 32 or 64 and
+    the padded rows and columns stay exactly zero)."""
     Np = padded_dimension(N)
+    return 64 if tensor_cores and Np == 48 else Np
+
+
+def decompose(model, sweep_symbols, cache_key, tile=None):
+    """:class:`MatrixModel` of a model prepared by :func:`gqis.rhs.prepare_model` (``tile``: the padded
+    dimension, :func:`padded_dimension` when None)."""
+    N = int(model["N"])
+    Np = padded_dimension(N) if tile is None else int(tile)
     # Constant-only subexpressions that prepare_model named (ConstExpr_k, x__sqrt ...) are put
     # back: the split below needs sqrt(G)/2 and -sqrt(G)/2 to share the factor sqrt(G).
     base = tuple(model["base_runtime_syms"])
@@ -267,8 +276,9 @@ def decompose(model, sweep_symbols, cache_key):
 
 def compile_matrix_model(H, Drive, Col_Ops, mean_operator, *, sweep_symbols, const_values=None,
                          runtime_consts=None, keep_symbolic_consts=None, auto_runtime_consts=False,
-                         rho0=None, reuse=True):
-    """Prepare a model for the matrix form; returns ``(MatrixModel, "hit" | "miss")``."""
+                         rho0=None, reuse=True, tensor_cores=False):
+    """Prepare a model for the matrix form; returns ``(MatrixModel, "hit" | "miss")``.
+    ``tensor_cores``: pad for the tensor-core kernel (:func:`tile_dimension`)."""
     model = prepare_model(H, Drive, Col_Ops, mean_operator, sweep_symbols=tuple(sweep_symbols),
                           const_values=const_values, runtime_consts=runtime_consts,
                           keep_symbolic_consts=keep_symbolic_consts, auto_runtime_consts=auto_runtime_consts,
@@ -279,11 +289,14 @@ def compile_matrix_model(H, Drive, Col_Ops, mean_operator, *, sweep_symbols, con
            tuple(sp.srepr(L) for L in model["Col_Ops"]), sp.srepr(model["mean_operator"]),
            tuple(str(s) for s in model["runtime_const_syms"]),
            None if model["rho0_exprs"] is None else tuple(sp.srepr(e) for e in model["rho0_exprs"]))
+    tile = tile_dimension(int(model["N"]), tensor_cores)
+    if tile != padded_dimension(int(model["N"])):
+        key = key + (("tile", tile),)
     if reuse and key in _CACHE:
         return _CACHE[key], "hit"
     mm = _disk_load(key) if reuse else None
     if mm is None:
-        mm = decompose(model, sweep_symbols, key)
+        mm = decompose(model, sweep_symbols, key, tile)
         if reuse:
             _disk_store(key, mm)
     if reuse:

@@ -3,10 +3,16 @@
 Requests - any ``mesolve_2D`` / ``odesolve_2D`` call, of any model, size, integrator or form - are
 admitted while device memory and slots allow, split into point chunks, and their chunks are
 interleaved across several CUDA streams, so work of requests that arrive while others run overlaps
-on the device. Inputs and outputs stay resident in device memory from admission to completion;
-adaptive requests keep work stealing inside each chunk. The server loop is one host thread; every
-launch goes through the model module's C ABI (``gqis_sweep_launch``), a chunk being the descriptor's
-``[point_begin, point_begin + point_count)`` slice with per-point pointers offset to that slice.
+on the device. Inputs and outputs stay resident in device memory from admission to completion.
+The server loop is one host thread; every launch goes through the model module's C ABI
+(``gqis_sweep_launch``), a chunk being the descriptor's ``[point_begin, point_begin + point_count)``
+slice with per-point pointers offset to that slice.
+
+Adaptive requests steal work across requests: each dispatch pass gathers the next chunk of every
+admitted adaptive request of the same module into one ``gqis_sweep_launch_batch`` grid, whose
+persistent lanes take points of all those chunks from one counter. Points whose step counts differ
+no longer leave a request's launch idle behind its slowest point: other requests' points fill the
+lanes that finish early.
 
 Each point's result depends only on its own inputs, so a request returns the same values alone and
 in the mix (the GPU tests check that bit for bit).
@@ -27,6 +33,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 QUEUED, RUNNING, DONE, FAILED, CANCELLED = "queued", "running", "done", "failed", "cancelled"
+BATCH_MAX = 64  # sweeps per gqis_sweep_launch_batch grid (GQIS_BATCH_MAX)
 
 
 class SweepFuture:
@@ -209,6 +216,25 @@ class TorchBackend:
         ev.record(st)
         return ev
 
+    def launch_batch(self, items, stream_index):
+        """One grid for chunks of several adaptive requests of one module (``items``: (request, chunk)
+        pairs); their lanes share one fresh work counter. Returns the event and the counter, which
+        must stay alive until the event completes."""
+        from . import abi
+        torch = self.torch
+        st = self.streams[stream_index]
+        for req, _ in items:
+            st.wait_event(req.handle["ready"])
+        with torch.cuda.device(self.device), torch.cuda.stream(st):
+            counter = torch.zeros(1, dtype=torch.int32, device=self.device)
+        descs = (abi.SweepDesc * len(items))(*[chunk for _, chunk in items])
+        lib = items[0][0].handle["module"].lib
+        rc = lib.gqis_sweep_launch_batch(descs, len(items), counter.data_ptr(), st.cuda_stream)
+        abi.check(rc, lib)
+        ev = torch.cuda.Event()
+        ev.record(st)
+        return ev, counter
+
     @staticmethod
     def query(event):
         return event.query()
@@ -260,8 +286,9 @@ class SweepServer:
         self._used = 0
         self._stop = False
         self._stream_load = [0] * self.nstreams
+        self._batches = hasattr(self.backend, "launch_batch")  # cross-request batches of adaptive chunks
         self.stats = {"submitted": 0, "completed": 0, "failed": 0, "cancelled": 0, "point_steps": 0,
-                      "max_concurrent": 0}
+                      "max_concurrent": 0, "batched_launches": 0}
         self._thread = threading.Thread(target=self._loop, name="gqis-serve", daemon=True)
         self._thread.start()
 
@@ -401,8 +428,12 @@ class SweepServer:
             oldest = min(self._active, key=lambda r: r.future.id)
             order.remove(oldest)
             order.insert(0, oldest)
+        batched = {}  # adaptive requests by module: their next chunks go out as one grid
         for req in order:
             if req.cancel or not req.chunks or req.copying is not None:
+                continue
+            if self._batches and req.kind == "sweep" and getattr(req.launch, "adaptive", False):
+                batched.setdefault(str(req.handle["module"].path), []).append(req)
                 continue
             s = min(range(self.nstreams), key=lambda i: self._stream_load[i])
             if self._stream_load[s] >= 2:
@@ -415,7 +446,26 @@ class SweepServer:
                 req.future.error = repr(exc)
                 continue
             self._stream_load[s] += 1
-            req.inflight.append((ev, s))
+            req.inflight.append((ev, s, {}))
+            progressed = True
+        for reqs in batched.values():
+            s = min(range(self.nstreams), key=lambda i: self._stream_load[i])
+            if self._stream_load[s] >= 2:
+                break
+            reqs = reqs[:BATCH_MAX]
+            items = [(req, req.chunks.popleft()) for req in reqs]
+            try:
+                ev, keep = self.backend.launch_batch(items, s)
+            except Exception as exc:  # a rejected batch fails its requests only
+                for req in reqs:
+                    req.cancel = True
+                    req.future.error = repr(exc)
+                continue
+            self._stream_load[s] += 1
+            token = {"keep": keep}  # one launch: the stream load is released once
+            for req in reqs:
+                req.inflight.append((ev, s, token))
+            self.stats["batched_launches"] += 1
             progressed = True
         return progressed
 
@@ -423,12 +473,15 @@ class SweepServer:
         progressed = False
         for req in list(self._active):
             still = []
-            for ev, s in req.inflight:
+            for ev, s, token in req.inflight:
                 if self.backend.query(ev):
-                    self._stream_load[s] -= 1
+                    if not token.get("done"):
+                        token["done"] = True
+                        token.pop("keep", None)
+                        self._stream_load[s] -= 1
                     progressed = True
                 else:
-                    still.append((ev, s))
+                    still.append((ev, s, token))
             req.inflight = still
             if req.inflight:
                 continue

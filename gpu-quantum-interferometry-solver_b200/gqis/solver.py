@@ -613,9 +613,10 @@ def _solve_symbolic_system(H, Drive, Col_Ops, mean_operator, tlist,
             compiled, rhs_status = matrix_form.compile_matrix_model(
                 H, Drive, Col_Ops, mean_operator, sweep_symbols=tuple(var_arrays), const_values=const_values,
                 runtime_consts=runtime_consts, keep_symbolic_consts=keep_symbolic_consts,
-                auto_runtime_consts=auto_runtime_consts, rho0=rho0, reuse=RHSreuse)
+                auto_runtime_consts=auto_runtime_consts, rho0=rho0, reuse=RHSreuse,
+                tensor_cores=form == "fp32" and rhs_form in ("auto", "matrix_tc"))
         if rhs_form == "auto" and not matrix_form.tensor_core_blockers(compiled, form):
-            tensor_cores = True  # FP32 sweeps of N = 16 .. 32 run on the tensor cores
+            tensor_cores = True  # FP32 sweeps from N = 8 run on the tensor cores
     elif compiled_rhs is None:
         compiled, rhs_status = _compile_rhs(
             H, Drive, Col_Ops, mean_operator, sweep_symbols=tuple(var_arrays), const_values=const_values,

@@ -171,3 +171,17 @@ def test_two_cta_tensor_core_kernel_records_the_trace():
     assert float(np.max(np.abs(ref_tr))) > 1e-4  # the top level's population grows to ~1e-3 by t = 5
     assert float(np.max(np.abs(got_tr - ref_tr))) <= 5e-6
     assert float(np.max(np.abs(got_map - ref_map))) <= 5e-6
+
+
+@pytest.mark.gpu
+def test_dimension_40_runs_on_the_tensor_cores_padded_to_64():
+    """A model of dimension 33 .. 48 pads to 64 for the tensor-core kernel (its rows and columns past
+    N stay zero), while the FP64 CUDA-core form keeps the 48-wide tile: both equal the oracle."""
+    import gqis
+    w, args, kwargs = hilbert_model(40)
+    tc, info = gqis.mesolve_2D(*args, **kwargs, precision="fp32", return_timing_info=True)
+    assert info["rhs_form"] == "matrix_tc"
+    fp64 = gqis.mesolve_2D(*args, **kwargs, fp64=True, rhs_form="matrix")
+    ref = _oracle(w, kwargs)
+    assert float(np.max(np.abs(fp64 - ref))) <= 1e-11
+    assert float(np.max(np.abs(tc - ref))) <= 2e-6

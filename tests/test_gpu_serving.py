@@ -34,6 +34,32 @@ def test_each_request_is_the_same_alone_and_in_the_mix():
 
 
 @pytest.mark.gpu
+def test_adaptive_requests_share_batched_grids_and_match_their_direct_calls():
+    """Adaptive requests of one module (here three Duffing sweeps of different grids and tolerances)
+    are served by batch launches whose lanes take points of every request from one counter; each
+    request's final states, traces and step counts equal its direct call bit for bit."""
+    import gqis
+    from gqis.serving import SweepServer
+    from test_support_calls import duffing_case
+    calls = []
+    for side, rtol in ((8, 1e-8), (12, 1e-7), (5, 1e-9)):
+        _, args, kwargs = duffing_case(side=side, solver="tsit5a")
+        kwargs["adaptive_options"] = dict(kwargs["adaptive_options"], step_rtol=rtol)
+        calls.append((args, kwargs))
+    alone = [gqis.odesolve_2D(*a, **kw, return_timing_info=True) for a, kw in calls]
+    with SweepServer(streams=2, chunk_points=40, max_inflight=8) as srv:
+        futs = [srv.submit("odesolve_2D", *a, **kw) for a, kw in calls]
+        outs = [f.result(300) for f in futs]
+        stats = dict(srv.stats)
+    assert stats["batched_launches"] >= 1 and stats["completed"] == len(calls)
+    for (final, trace, _, info), out in zip(alone, outs):
+        np.testing.assert_array_equal(out["result"], final)
+        np.testing.assert_array_equal(out["trace"], trace)
+        counts = np.stack([info["adaptive_steps"]["accepted"], info["adaptive_steps"]["rejected"]], -1)
+        np.testing.assert_array_equal(out["step_counts"].reshape(counts.shape), counts)
+
+
+@pytest.mark.gpu
 def test_server_isolates_a_request_the_c_abi_rejects():
     """A launch the module rejects (status != 0) fails its own request; the others complete."""
     import dataclasses

@@ -54,6 +54,9 @@ def matrix_calls():
     for N in (16, 64):
         _, args, kwargs = hilbert_model(N)
         out.append(("mesolve_2D", args, dict(kwargs, precision="fp32", rhs_form="matrix_tc", output_mode="final_rho")))
+    _, args, kwargs = hilbert_model(40)  # a dimension of 33 .. 48: 48-wide CUDA-core tile, 64 on the tensor cores
+    out.append(("mesolve_2D", args, dict(kwargs, fp64=True, rhs_form="matrix")))
+    out.append(("mesolve_2D", args, dict(kwargs, precision="fp32")))
     _, args, kwargs = hilbert_model(16)  # the give-up path of the tensor-core kernel's MMA waits
     out.append(("mesolve_2D", args, dict(kwargs, precision="fp32", rhs_form="matrix_tc", nvrtc_options=GIVE_UP)))
     _, args, kwargs = hilbert_model(64)  # the two-CTA tensor-core kernel's trace against the FP64 matrix form
