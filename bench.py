@@ -219,7 +219,10 @@ def run_ours(args):
     a_axis = np.linspace(0.0, 5.0, side)
     call = dict(var_arrays={eps: eps_axis, A: a_axis}, const_values={})
     model = (w["H"], w["Drive"], w["Col_Ops"], w["mean_operator"], w["tlist"])
-    fp32 = solver.prepare_sweep("mesolve_2D", *model, **call, precision="fp32")
+    # the FP32 form's kernel: two points per thread in packed f32x2 arithmetic (the default for this
+    # model), or one point per thread (--fp32-kernel scalar, for comparison)
+    kernel_flags = ("-DGQ_PACK2=0",) if args.fp32_kernel == "scalar" else ()
+    fp32 = solver.prepare_sweep("mesolve_2D", *model, **call, precision="fp32", nvrtc_options=kernel_flags)
     fp64 = solver.prepare_sweep("mesolve_2D", *model, **call, precision="fp64")
     flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
     points, ksteps = fp32.points, fp32.steps
@@ -251,7 +254,7 @@ def run_ours(args):
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
-        out = gqis.mesolve_2D(*model, **call, fp64=False)
+        out = gqis.mesolve_2D(*model, **call, fp64=False, nvrtc_options=kernel_flags)
         b.record()
         b.synchronize()
         if k >= args.warmup:
@@ -275,7 +278,9 @@ def run_ours(args):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": dict(four_level_config(side, ksteps, ws),
                            l2="flushed (256 MiB write) between timed launches",
-                           form="FP32 state/RHS, FP64 time + drive phase + compensated average"),
+                           form="FP32 state/RHS, FP64 time + drive phase + compensated average",
+                           fp32_kernel=("two points per thread, packed f32x2" if args.fp32_kernel == "packed"
+                                        else "one point per thread")),
             "plain_fp64": {"value": total_units / (ms64 / 1e3), "ms_per_step": ms64},
             "speedup_vs_plain_fp64": ms64 / ms32,
             "max_abs_err_vs_fp64": err,
@@ -874,6 +879,8 @@ def main():
     ap.add_argument("--side", type=int, default=SIDE)
     ap.add_argument("--nsteps", type=int, default=NSTEPS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fp32-kernel", default="packed", choices=("packed", "scalar"),
+                    help="four_level: the FP32 form's kernel (two points per thread, or one)")
     ap.add_argument("--reference-gpu", action="store_true",
                     help="also time the reference's generated kernels on this GPU")
     ap.add_argument("--requests", type=int, default=48, help="serving: number of requests")

@@ -8,7 +8,10 @@
 //              least-loaded stream, at most two chunks queued per stream; a chunk is the caller's
 //              descriptor restricted to [point_begin + b, point_begin + b + n) with the per-point
 //              pointers (results, rho0, trace, step_counts) offset to that slice, and for the
-//              adaptive integrators a zeroed work counter of its own;
+//              adaptive integrators a zeroed work counter of its own. The next chunks of all
+//              running adaptive requests of one module go out together as one batch grid
+//              (gqis_sweep_launch_batch, one zeroed counter): the persistent lanes take points of
+//              every request from that counter, so work is stolen across requests;
 //   complete - chunks end when their event has completed; a request ends when its last chunk has.
 // A launch the module rejects fails its own request only (with the module's error text).
 // Host threads submit, poll, wait and cancel under one mutex.
@@ -43,20 +46,29 @@ int fail(int code, const char* fmt, ...) {
 }
 
 using launch_fn = int (*)(const gqis_sweep_desc*, void*);
+using batch_fn = int (*)(const gqis_sweep_desc*, int32_t, uint32_t*, void*);
 using info_fn = int (*)(gqis_model_info*);
 using error_fn = const char* (*)(void);
 
 struct Module {
     void* handle = nullptr;
     launch_fn launch = nullptr;
+    batch_fn batch = nullptr;  // gqis_sweep_launch_batch (absent from older modules)
     error_fn last_error = nullptr;
     gqis_model_info info{};
 };
 
-struct InFlight {
+// One launch on the device. A batch launch is shared by the requests whose chunks it carries: its
+// event, stream slot and counter are released when the last of them has seen it complete.
+struct Launch {
     cudaEvent_t event;
     int stream;
     int counter;  // index into the server's work counters, or -1
+    int holders;  // requests still holding this launch
+};
+
+struct InFlight {
+    std::shared_ptr<Launch> launch;
 };
 
 struct Request {
@@ -107,6 +119,7 @@ struct gqis_server {
         auto m = std::make_unique<Module>();
         m->handle = h;
         m->launch = reinterpret_cast<launch_fn>(dlsym(h, "gqis_sweep_launch"));
+        m->batch = reinterpret_cast<batch_fn>(dlsym(h, "gqis_sweep_launch_batch"));
         m->last_error = reinterpret_cast<error_fn>(dlsym(h, "gqis_last_error"));
         info_fn info = reinterpret_cast<info_fn>(dlsym(h, "gqis_model_info_get"));
         if (!m->launch || !m->last_error || !info) {
@@ -172,13 +185,55 @@ struct gqis_server {
         return d;
     }
 
+    int least_loaded() const {
+        int s = 0;
+        for (int i = 1; i < nstreams; ++i)
+            if (load[i] < load[s]) s = i;
+        return s;
+    }
+
+    // The next chunk of each request in rs (adaptive, one module) as one batch grid on stream s.
+    void dispatch_batch(Module* m, const std::vector<std::shared_ptr<Request>>& rs, int s) {
+        std::vector<gqis_sweep_desc> ds;
+        for (const auto& r : rs) {
+            const auto chunk = r->chunks.front();
+            r->chunks.pop_front();
+            ds.push_back(chunk_desc(*r, chunk.first, chunk.second));
+        }
+        const int counter = free_counters.back();
+        free_counters.pop_back();
+        cudaMemsetAsync(counters + counter, 0, sizeof(unsigned int), streams[s]);
+        const int rc = m->batch(ds.data(), (int32_t)ds.size(), counters + counter, streams[s]);
+        if (rc != GQIS_OK) {
+            for (const auto& r : rs) {
+                r->error = m->last_error();
+                r->cancel = true;
+            }
+            free_counters.push_back(counter);
+            return;
+        }
+        cudaEvent_t ev;
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventRecord(ev, streams[s]) != cudaSuccess) {
+            cudaStreamSynchronize(streams[s]);  // no event: wait here instead
+            free_counters.push_back(counter);
+            return;
+        }
+        load[s] += 1;
+        auto launch = std::make_shared<Launch>(Launch{ev, s, counter, (int)rs.size()});
+        for (const auto& r : rs) r->inflight.push_back({launch});
+    }
+
     bool dispatch() {
         bool progressed = false;
+        std::map<Module*, std::vector<std::shared_ptr<Request>>> batched;  // adaptive requests by module
         for (auto& r : std::vector<std::shared_ptr<Request>>(active)) {
             if (r->cancel || r->chunks.empty()) continue;
-            int s = 0;
-            for (int i = 1; i < nstreams; ++i)
-                if (load[i] < load[s]) s = i;
+            if (adaptive(r->module->info) && r->module->batch) {
+                batched[r->module].push_back(r);
+                continue;
+            }
+            const int s = least_loaded();
             if (load[s] >= 2) break;
             const auto chunk = r->chunks.front();
             r->chunks.pop_front();
@@ -207,7 +262,15 @@ struct gqis_server {
                 continue;
             }
             load[s] += 1;
-            r->inflight.push_back({ev, s, counter});
+            r->inflight.push_back({std::make_shared<Launch>(Launch{ev, s, counter, 1})});
+            progressed = true;
+        }
+        for (auto& group : batched) {
+            const int s = least_loaded();
+            if (load[s] >= 2 || free_counters.empty()) break;
+            std::vector<std::shared_ptr<Request>>& rs = group.second;
+            if (rs.size() > (size_t)GQIS_BATCH_MAX) rs.resize(GQIS_BATCH_MAX);
+            dispatch_batch(group.first, rs, s);
             progressed = true;
         }
         return progressed;
@@ -218,7 +281,8 @@ struct gqis_server {
         for (auto& r : std::vector<std::shared_ptr<Request>>(active)) {
             std::vector<InFlight> still;
             for (const InFlight& f : r->inflight) {
-                const cudaError_t q = cudaEventQuery(f.event);
+                Launch& l = *f.launch;
+                const cudaError_t q = cudaEventQuery(l.event);
                 if (q == cudaErrorNotReady) {
                     still.push_back(f);
                     continue;
@@ -227,9 +291,11 @@ struct gqis_server {
                     r->error = std::string("chunk failed on the device: ") + cudaGetErrorString(q);
                     r->cancel = true;
                 }
-                cudaEventDestroy(f.event);
-                load[f.stream] -= 1;
-                if (f.counter >= 0) free_counters.push_back(f.counter);
+                if (--l.holders == 0) {  // the last request of a shared batch releases its launch
+                    cudaEventDestroy(l.event);
+                    load[l.stream] -= 1;
+                    if (l.counter >= 0) free_counters.push_back(l.counter);
+                }
                 progressed = true;
             }
             r->inflight.swap(still);

@@ -1,4 +1,5 @@
-"""The native sweep server (include/gqis_serve.h) on the GPU: requests of three kernel kinds submitted
+"""The native sweep server (include/gqis_serve.h) on the GPU: requests of three kernel kinds (two adaptive
+requests of one module, whose chunks go out as shared batch grids) submitted
 together through the C ABI, cut into 97-point chunks on three streams, give the results of their
 direct launches bit for bit; a request its module rejects fails alone with the module's message."""
 
@@ -31,6 +32,9 @@ def _sweeps():
     for name in ("c2_fp64_mean_sub32", "duffing_tsit5a_trace"):  # fixed-step; adaptive with a trace
         c = cases[name]
         out[name] = solver.prepare_sweep(c["api"], *c["args"], **c["kwargs"])
+    # a second request of the same adaptive module: its chunks share batch grids with the first's
+    c = cases["duffing_tsit5a_trace"]
+    out["duffing_part"] = solver.prepare_sweep(c["api"], *c["args"], **c["kwargs"], point_begin=5, point_count=101)
     _, args, kwargs = hilbert_model(16, side=(12, 9))  # tensor cores: 8-point tiles split by the chunks
     out["tc16"] = solver.prepare_sweep("mesolve_2D", *args, **dict(kwargs, precision="fp32", rhs_form="matrix_tc"))
     return out
