@@ -5,11 +5,15 @@
 // (N = padded dimension 8, 16, 32 or 64) is one M = 128 MMA:
 //
 //   row r = p*N + j  (point p of the tile, column j of its rho)  = tensor-memory lane r
-//   A[r][k]   = Re rho_p[k][j] (k < N),  Im rho_p[k-N][j] (k >= N)        (tensor memory)
+//   A[r][k]   = Re rho_p[m][j] (k = 2m),  Im rho_p[m][j] (k = 2m + 1)     (tensor memory)
 //   B[k][col] = real embedding of T_q^T for the operator terms           (shared memory)
 //               T_0 = Heff0, T_q = M_q (dense, q = 1..ND), T_{ND+g} = diag(v_g) (g = 1..NG)
-//               col = (2q + c) NH + n - nb, c = 0 (Re) / 1 (Im)
-//   D[r][col] = Re/Im (T_q rho_p)[n][j]                                    (tensor memory)
+//               col = 2 NH q + 2 (n - nb) + c, c = 0 (Im) / 1 (Re)
+//   D[r][col] = Im/Re (T_q rho_p)[n][j]                                    (tensor memory)
+//
+// Real and imaginary parts sit in adjacent columns, so one 32x32b load or store moves a thread's E
+// complex elements as (Im, Re) or (Re, Im) register pairs, on which the epilogue computes in packed
+// FP32 (one f32x2 instruction per complex element; each lane rounds as the scalar instruction).
 //
 // Up to N = 32 one CTA holds the tile (NH = N rows n of every column, nb = 0). At N = 64 the
 // tile's state does not fit one SM's registers, so a cluster of CL = 2 CTAs shares it: CTA c owns
@@ -46,6 +50,7 @@
 
 #include <type_traits>
 
+#include "gqis_f32x2.cuh"
 #include "gqis_matrix.cuh"
 #include "gqis_tcgen05.cuh"
 
@@ -53,6 +58,9 @@ namespace gqmatrix_tc {
 
 using gqmatrix::Cx;
 using gqmatrix::ldc;
+using gq::f2_add;
+using gq::f2_fma;
+using gq::f2_sub;
 
 // mbarrier polls before an in-loop wait (MMA completion, partner's bytes) gives up. A build can
 // lower it (-DGQ_TC_MAX_POLLS=0 makes every such wait give up at once, which tests the give-up
@@ -63,6 +71,11 @@ using gqmatrix::ldc;
 #endif
 constexpr uint32_t kMaxPolls = GQ_TC_MAX_POLLS;
 constexpr uint32_t kDrainPolls = 1u << 20;
+
+// Tensor-memory columns an allocation of `used` columns takes (a power of two, at least 32).
+__host__ __device__ constexpr int tmem_alloc_cols(int used) {
+    return used <= 32 ? 32 : used <= 64 ? 64 : used <= 128 ? 128 : used <= 256 ? 256 : 512;
+}
 
 template <class MM>
 struct TcShape {
@@ -85,12 +98,13 @@ struct TcShape {
     static constexpr int TS = 3 * KB;         // table slots per block: start, midpoint and end of each step
     static constexpr int COL_D = 0, COL_AHI = NMMA, COL_ALO = NMMA + KDIM;
     static constexpr int COLS_USED = NMMA + 2 * KDIM;
-    static constexpr int TMEM_COLS = COLS_USED <= 32 ? 32 : COLS_USED <= 64 ? 64 : COLS_USED <= 128 ? 128
-                                   : COLS_USED <= 256 ? 256 : 512;
+    static constexpr uint32_t KSTEP_BYTES = 2u * NMMA * 32u;  // B of one K step: NMMA hi rows, then NMMA lo rows
+    static constexpr int TMEM_COLS = tmem_alloc_cols(COLS_USED);
     static constexpr int LDK = N + 2;         // padded column stride of the K buffer (16-byte rows, no conflicts)
+    static_assert(2 * E <= 16, "one 32x32b.x16 tensor-memory access per operand pair block");
     // shared memory layout (bytes)
-    static constexpr size_t B_BYTES = (size_t)NMMA * KDIM * 4;
-    static constexpr size_t OFF_BHI = 0, OFF_BLO = B_BYTES;
+    static constexpr size_t B_BYTES = (size_t)NMMA * KDIM * 4;  // one of the two TF32 parts
+    static constexpr size_t OFF_B = 0;
     static constexpr size_t OFF_K = 2 * B_BYTES;
     static constexpr size_t K_BYTES = (size_t)P * NH * LDK * 8;  // K[j][n] for the CTA's rows n, every j
     static constexpr size_t OFF_X = OFF_K + K_BYTES;            // [P][H][E/2][N] x 2 the partner's stage input
@@ -102,7 +116,9 @@ struct TcShape {
     static constexpr size_t CS_BYTES = 2 * (size_t)TS * P * NC * 4;
     static constexpr size_t OFF_RED = (OFF_CS + CS_BYTES + 7) / 8 * 8;
     static constexpr size_t RED_BYTES = 2 * (size_t)H * CG * P * 8 + 2 * (size_t)P * 8;  // + the partner's sums
-    static constexpr size_t OFF_MISC = OFF_RED + RED_BYTES;     // mbarriers, tensor-memory slot, failure flag
+    static constexpr size_t OFF_DV = OFF_RED + RED_BYTES;       // [P][N] sum_g c_g v_g[n] of the stage
+    static constexpr size_t DV_BYTES = (NGM < MM::NG) ? (size_t)P * N * 8 : 0;
+    static constexpr size_t OFF_MISC = OFF_DV + DV_BYTES;       // mbarriers, tensor-memory slot, failure flag
     static constexpr size_t NEEDED = OFF_MISC + 64;
     // At most 512 / TMEM_COLS CTAs can hold tensor memory on one SM: pad the shared memory so that
     // no more CTAs fit (228 KB per SM, 1 KB reserved per CTA) and no allocation ever waits.
@@ -118,11 +134,13 @@ struct TcShape {
     static_assert(MIN_CTAS >= 1, "threads");
 };
 
-// Byte offset of B element (col, k) in the K-major no-swizzle layout: per K step of 8, rows in
-// groups of 8 (256 bytes: two 8 x 16-byte core matrices for the K halves).
+// Byte offset of B element (col, k) of TF32 part `part` (0 hi, 1 lo) in the K-major no-swizzle layout:
+// per K step of 8 the hi rows, then the lo rows, in groups of 8 (256 bytes: two 8 x 16-byte core
+// matrices for the K halves).
 template <class T>
-__device__ __forceinline__ uint32_t b_offset(int col, int k) {
-    return (uint32_t)((k >> 3) * (T::NMMA * 32) + (col >> 3) * 256 + ((k & 7) >> 2) * 128 + (col & 7) * 16 + (k & 3) * 4);
+__device__ __forceinline__ uint32_t b_offset(int col, int k, int part) {
+    return (uint32_t)((k >> 3) * T::KSTEP_BYTES + part * (T::NMMA * 32) + (col >> 3) * 256 + ((k & 7) >> 2) * 128 +
+                      (col & 7) * 16 + (k & 3) * 4);
 }
 
 // TF32 rounding (nearest, ties away from zero) of a finite FP32 number with integer operations:
@@ -134,17 +152,16 @@ __device__ __forceinline__ float tf32_round(float x) {
 template <class MM, int OUT, int TRACE>
 __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) matrix_tc_kernel(const gqis_sweep_desc d) {
     using T = TcShape<MM>;
-    using F = FormFP32;
     constexpr int N = T::N, P = T::P, E = T::E, LDK = T::LDK, NO = MM::NO, NC = T::NC, NH = T::NH, H = T::H;
     static_assert(std::is_same<typename MM::real, float>::value, "tensor-core form uses FP32 model data");
     extern __shared__ __align__(1024) unsigned char gq_smem[];
-    float* const bhi = reinterpret_cast<float*>(gq_smem + T::OFF_BHI);
-    float* const blo = reinterpret_cast<float*>(gq_smem + T::OFF_BLO);
-    Cx<float>* const kbuf = reinterpret_cast<Cx<float>*>(gq_smem + T::OFF_K);
+    float* const bsm = reinterpret_cast<float*>(gq_smem + T::OFF_B);
+    float2* const kbuf = reinterpret_cast<float2*>(gq_smem + T::OFF_K);  // (Im, Re) of K[n][j]
     float2* const xbuf = reinterpret_cast<float2*>(gq_smem + T::OFF_X);
     float* const rdiag = reinterpret_cast<float*>(gq_smem + T::OFF_RD);
     float* const cs = reinterpret_cast<float*>(gq_smem + T::OFF_CS);
     double* const red = reinterpret_cast<double*>(gq_smem + T::OFF_RED);
+    Cx<float>* const dvs = reinterpret_cast<Cx<float>*>(gq_smem + T::OFF_DV);
     uint64_t* const bar = reinterpret_cast<uint64_t*>(gq_smem + T::OFF_MISC);
     uint32_t* const tslot = reinterpret_cast<uint32_t*>(gq_smem + T::OFF_MISC + 8);
     uint32_t* const fail_flag = reinterpret_cast<uint32_t*>(gq_smem + T::OFF_MISC + 12);  // set by the partner
@@ -170,9 +187,10 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
     // ---- B = split-TF32 real embedding of the operator terms; mbarrier; tensor memory
     for (int e = tid; e < T::NMMA * T::KDIM; e += T::THREADS) {
         const int col = e / T::KDIM, k = e % T::KDIM;
-        const int q = col / (2 * NH), c = (col / NH) & 1, n = nb + col % NH;
-        const int m = k % N;
-        const bool imag_in = k >= N;
+        const int q = col / (2 * NH), n = nb + (col % (2 * NH)) / 2;
+        const bool re_out = (col & 1) != 0;  // output columns (Im, Re) of row n
+        const int m = k >> 1;
+        const bool imag_in = (k & 1) != 0;   // input columns (Re, Im) of row m
         float tr, ti;
         if (q <= MM::ND) {  // Heff0 and the dense terms; then the diagonal terms (NGM of them)
             const float* op = (q == 0) ? MM::heff() : MM::dense(q - 1);
@@ -183,12 +201,12 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
             tr = (n == m) ? __ldg(v + 2 * n) : 0.f;
             ti = (n == m) ? __ldg(v + 2 * n + 1) : 0.f;
         }
-        const float val = (c == 0) ? (imag_in ? -ti : tr) : (imag_in ? tr : ti);
+        // Re out = sum Tr Re rho - Ti Im rho; Im out = sum Ti Re rho + Tr Im rho
+        const float val = re_out ? (imag_in ? -ti : tr) : (imag_in ? tr : ti);
         const float hi = tf32_round(val);
         const float lo = tf32_round(val - hi);
-        const uint32_t off = b_offset<T>(col, k) >> 2;
-        bhi[off] = hi;
-        blo[off] = lo;
+        bsm[b_offset<T>(col, k, 0) >> 2] = hi;
+        bsm[b_offset<T>(col, k, 1) >> 2] = lo;
     }
     gqtc::fence_proxy_async_smem();
     if (tid == 0) {
@@ -215,10 +233,13 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
     const uint32_t t_ahi = tbase + T::COL_AHI + lane_base;
     const uint32_t t_alo = tbase + T::COL_ALO + lane_base;
     const uint32_t idesc = gqtc::idesc_tf32_m128(T::NMMA);
-    const uint32_t b_hi_addr = gqtc::smem_u32(bhi), b_lo_addr = gqtc::smem_u32(blo);
+    // B descriptor of K step 0; K step kc and the lo part are fixed offsets in its 14-bit address field
+    // (shared-memory addresses stay below 2^18 bytes)
+    const uint64_t bdesc0 = gqtc::smem_desc_kmajor(gqtc::smem_u32(bsm), 128, 256);
 
-    // ---- state: rows n0 .. n0 + E - 1 of column j, FP32 with compensation
-    float yre[E], yim[E], cre[E], cim[E], are[E], aim[E];
+    // ---- state: rows n0 .. n0 + E - 1 of column j as (Re, Im) pairs, FP32 with compensation (kept
+    // negated), and the RK4 sum of the step's stages
+    float2 y[E], cn[E], acc[E];
     {
         double pop_last = 1.0;
         if constexpr (MM::kInitFromArray) {
@@ -246,14 +267,14 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
                 vr = (float)v.re;
                 vi = (float)v.im;
             }
-            yre[e] = vr;
-            yim[e] = vi;
-            cre[e] = cim[e] = 0.f;
-            are[e] = aim[e] = 0.f;
+            y[e] = make_float2(vr, vi);
+            cn[e] = acc[e] = make_float2(0.f, 0.f);
         }
     }
     const int jl = j * (N / E) + n0 / E;  // this thread's jump list (column j, row block n0 / 8)
     const int jcount = __ldg(MM::tcj_count() + jl);
+    // every jump term feeds a diagonal element from a population: all of them are summed while the MMA runs
+    constexpr bool kJumpsEarly = MM::kJumpsOnDiagonal && !MM::kOwnTerms;
 
     const double dt = d.dt, dt2d = dt * 0.5;
     // Coefficient table of block b (steps b KB .. b KB + KB - 1) into buffer b & 1: for every point of
@@ -285,32 +306,32 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
         }
     };
 
-    // stage input u = y + s k -> A (hi / lo TF32 parts); populations -> rdiag[slot]; in a cluster
-    // also into the partner's exchange buffer (its rows of A are this CTA's rows)
-    auto write_stage = [&](float s, const float (&kre)[E], const float (&kim)[E], int slot) {
-        float hr[E], hi_[E], lr[E], li[E];
-        float pr = 0.f, pi = 0.f;  // the previous row's stage input
+    // stage input u = y + s k -> A (hi / lo TF32 parts, (Re, Im) column pairs); populations ->
+    // rdiag[slot]; in a cluster also into the partner's exchange buffer (its rows of A are this CTA's rows)
+    auto write_stage = [&](float s, const float2 (&k)[E], int slot) {
+        float hv[2 * E], lv[2 * E];
+        const float2 s2 = make_float2(s, s);
+        float2 prev = make_float2(0.f, 0.f);  // the previous row's stage input
 #pragma unroll
         for (int e = 0; e < E; ++e) {
-            const float ur = fmaf(s, kre[e], yre[e]), ui = fmaf(s, kim[e], yim[e]);
-            hr[e] = tf32_round(ur);
-            hi_[e] = tf32_round(ui);
-            lr[e] = ur - hr[e];  // |lo| <= 2^-11 |u|; its TF32 read loses at most 2^-21 |u|
-            li[e] = ui - hi_[e];
-            if (n0 + e == j) rdiag[slot * P * N + p * N + j] = ur;
+            const float2 u = f2_fma(s2, k[e], y[e]);
+            const float2 hi = make_float2(tf32_round(u.x), tf32_round(u.y));
+            const float2 lo = f2_sub(u, hi);  // |lo| <= 2^-11 |u|; its TF32 read loses at most 2^-21 |u|
+            hv[2 * e] = hi.x;
+            hv[2 * e + 1] = hi.y;
+            lv[2 * e] = lo.x;
+            lv[2 * e + 1] = lo.y;
+            if (n0 + e == j) rdiag[slot * P * N + p * N + j] = u.x;
             if constexpr (T::CL > 1) {  // rows e - 1, e as one 16-byte remote store
                 if (e & 1)
                     gqtc::st_async_v4(gqtc::cluster_peer_u32(xbuf, peer) +
                                           (uint32_t)((((p * H + hh) * (E / 2) + e / 2) * N + j) * 16),
-                                      pr, pi, ur, ui, gqtc::cluster_peer_u32(xbar, peer));
+                                      prev.x, prev.y, u.x, u.y, gqtc::cluster_peer_u32(xbar, peer));
             }
-            pr = ur;
-            pi = ui;
+            prev = u;
         }
-        gqtc::tmem_st<E>(t_ahi + n0, hr);
-        gqtc::tmem_st<E>(t_ahi + N + n0, hi_);
-        gqtc::tmem_st<E>(t_alo + n0, lr);
-        gqtc::tmem_st<E>(t_alo + N + n0, li);
+        gqtc::tmem_st<2 * E>(t_ahi + 2 * n0, hv);
+        gqtc::tmem_st<2 * E>(t_alo + 2 * n0, lv);
     };
 
     uint32_t phase = 0, xphase = 0, kphase = 0;
@@ -333,43 +354,32 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
     // k = f(u) for the stage input in A with the coefficients of table entry v; false when the MMA wait
     // gave up (one CTA; uniform over it). While the MMA runs, the threads fill the coefficient table of
     // block `fill` (if >= 0).
-    auto eval = [&](float (&kre)[E], float (&kim)[E], int slot, int v, int fill) -> bool {
+    auto eval = [&](float2 (&k)[E], int slot, int v, int fill) -> bool {
         if constexpr (T::CL > 1) {
             exchange_wait(xbar, xphase, (uint32_t)T::X_BYTES);  // the partner's half of the stage input
             const int mb = (crank ^ 1) * NH + hh * E;
             const float4* xs = reinterpret_cast<const float4*>(xbuf) + (p * H + hh) * (E / 2) * N + j;
-            float ur[E], ui[E];
+            float hv[2 * E], lv[2 * E];  // rows mb .. mb + E - 1 as (Re, Im) pairs
 #pragma unroll
             for (int e2 = 0; e2 < E / 2; ++e2) {
                 const float4 u = xs[e2 * N];
-                ur[2 * e2] = u.x;
-                ui[2 * e2] = u.y;
-                ur[2 * e2 + 1] = u.z;
-                ui[2 * e2 + 1] = u.w;
+                const float2 u0 = make_float2(u.x, u.y), u1 = make_float2(u.z, u.w);
+                const float2 h0 = make_float2(tf32_round(u0.x), tf32_round(u0.y));
+                const float2 h1 = make_float2(tf32_round(u1.x), tf32_round(u1.y));
+                const float2 l0 = f2_sub(u0, h0), l1 = f2_sub(u1, h1);
+                hv[4 * e2] = h0.x;
+                hv[4 * e2 + 1] = h0.y;
+                hv[4 * e2 + 2] = h1.x;
+                hv[4 * e2 + 3] = h1.y;
+                lv[4 * e2] = l0.x;
+                lv[4 * e2 + 1] = l0.y;
+                lv[4 * e2 + 2] = l1.x;
+                lv[4 * e2 + 3] = l1.y;
+                if (mb + 2 * e2 == j) rdiag[slot * P * N + p * N + j] = u0.x;
+                if (mb + 2 * e2 + 1 == j) rdiag[slot * P * N + p * N + j] = u1.x;
             }
-#pragma unroll
-            for (int e = 0; e < E; ++e)
-                if (mb + e == j) rdiag[slot * P * N + p * N + j] = ur[e];
-            {
-                float hv[E], lv[E];
-#pragma unroll
-                for (int e = 0; e < E; ++e) {
-                    hv[e] = tf32_round(ur[e]);
-                    lv[e] = ur[e] - hv[e];
-                }
-                gqtc::tmem_st<E>(t_ahi + mb, hv);
-                gqtc::tmem_st<E>(t_alo + mb, lv);
-            }
-            {
-                float hv[E], lv[E];
-#pragma unroll
-                for (int e = 0; e < E; ++e) {
-                    hv[e] = tf32_round(ui[e]);
-                    lv[e] = ui[e] - hv[e];
-                }
-                gqtc::tmem_st<E>(t_ahi + N + mb, hv);
-                gqtc::tmem_st<E>(t_alo + N + mb, lv);
-            }
+            gqtc::tmem_st<2 * E>(t_ahi + 2 * mb, hv);
+            gqtc::tmem_st<2 * E>(t_alo + 2 * mb, lv);
         }
         gqtc::tmem_wait_st();
         gqtc::fence_before_sync();
@@ -378,9 +388,8 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
             gqtc::fence_after_sync();
 #pragma unroll
             for (int kc = 0; kc < T::KCH; ++kc) {
-                const uint32_t boff = (uint32_t)(kc * T::NMMA * 32);
-                const uint64_t dh = gqtc::smem_desc_kmajor(b_hi_addr + boff, 128, 256);
-                const uint64_t dl = gqtc::smem_desc_kmajor(b_lo_addr + boff, 128, 256);
+                const uint64_t dh = bdesc0 + (uint64_t)((kc * T::KSTEP_BYTES) >> 4);
+                const uint64_t dl = dh + (uint64_t)((T::NMMA * 32) >> 4);
                 gqtc::mma_tf32_ts(tbase + T::COL_D, tbase + T::COL_AHI + 8 * kc, dh, idesc, kc > 0 ? 1u : 0u);
                 gqtc::mma_tf32_ts(tbase + T::COL_D, tbase + T::COL_AHI + 8 * kc, dl, idesc, 1u);
                 gqtc::mma_tf32_ts(tbase + T::COL_D, tbase + T::COL_ALO + 8 * kc, dh, idesc, 1u);
@@ -392,6 +401,37 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
         cq[0] = 1.f;
 #pragma unroll
         for (int q = 1; q < T::NT; ++q) cq[q] = cs[(v * P + p) * NC + (q - 1)];
+        // While the MMA runs: what needs no MMA result. The jump terms from populations (those of the
+        // stage input are in rdiag since the barrier above) and the diagonal terms' coefficients.
+        float jre = 0.f, jim = 0.f;
+        if constexpr (kJumpsEarly) {
+            // Every entry of the padded list (padding: weight 0, population 0), unrolled, so that all
+            // loads issue at once: the thread that issued the MMAs polls for them right after this.
+#pragma unroll
+            for (int q = 0; q < MM::TCJ_MAX; ++q) {
+                const int idx = jl * MM::TCJ_MAX + q;
+                const int rate = __ldg(MM::tcj_rate() + idx);
+                const Cx<float> w = ldc(MM::tcj_coef(), idx);
+                const float cr = (rate >= 0) ? cs[(v * P + p) * NC + (rate >= 0 ? rate : 0)] : 1.f;
+                const float x = rdiag[slot * P * N + p * N + __ldg(MM::tcj_a() + idx)];
+                jre = fmaf(w.re * cr, x, jre);
+                jim = fmaf(w.im * cr, x, jim);
+            }
+        }
+        if constexpr (T::NGM < MM::NG) {  // every point's sum_g c_g v_g[n], read after the barrier below
+            for (int idx = tid; idx < P * N; idx += T::THREADS) {
+                const int pp = idx / N, n = idx - pp * N;
+                Cx<float> dv = {0.f, 0.f};
+#pragma unroll
+                for (int g = 0; g < MM::NG; ++g) {
+                    const Cx<float> vg = ldc(MM::diag(g), n);
+                    const float cg = cs[(v * P + pp) * NC + MM::ND + g];
+                    dv.re = fmaf(cg, vg.re, dv.re);
+                    dv.im = fmaf(cg, vg.im, dv.im);
+                }
+                dvs[idx] = dv;
+            }
+        }
         // one thread polls the mbarrier; the others wait at the barrier instead of spinning
         const bool ok = (tid != 0) || failed || gqtc::mbar_wait_bounded(bar, phase, kMaxPolls);
         const bool bad = __syncthreads_or(!ok);  // MMA complete (or given up, uniformly over the CTA)
@@ -402,50 +442,41 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
             failed = true;
             mma_lost = true;
         }
-        float Kr[E], Ki[E], ur[E], ui[E];
+        float2 W[E];  // (Im, Re) of K[n][j] = sum_q c_q (T_q rho)[n][j] for the thread's rows n
+        float2 U[E];  // (Re, Im) of the stage input u[n][j], where a term needs it
 #pragma unroll
-        for (int e = 0; e < E; ++e) Kr[e] = Ki[e] = 0.f;
+        for (int e = 0; e < E; ++e) W[e] = U[e] = make_float2(0.f, 0.f);
         if (!failed) {  // (a cluster CTA that gave up sends zeros)
             phase ^= 1u;
             gqtc::fence_after_sync();
 #pragma unroll
             for (int q = 0; q < T::NT; ++q) {
-                float a[E], b[E];
-                gqtc::tmem_ld<E>(t_d + (2 * q) * NH + (n0 - nb), a);
-                gqtc::tmem_ld<E>(t_d + (2 * q + 1) * NH + (n0 - nb), b);
+                float dq[2 * E];
+                gqtc::tmem_ld<2 * E>(t_d + 2 * (q * NH + (n0 - nb)), dq);
                 gqtc::tmem_wait_ld();
+                const float2 c2 = make_float2(cq[q], cq[q]);
 #pragma unroll
                 for (int e = 0; e < E; ++e) {
-                    Kr[e] = (q == 0) ? a[e] : fmaf(cq[q], a[e], Kr[e]);
-                    Ki[e] = (q == 0) ? b[e] : fmaf(cq[q], b[e], Ki[e]);
+                    const float2 d2 = make_float2(dq[2 * e], dq[2 * e + 1]);
+                    W[e] = (q == 0) ? d2 : f2_fma(c2, d2, W[e]);
                 }
             }
             if constexpr (MM::kOwnTerms || (T::NGM < MM::NG)) {  // terms that need the stage input itself
-                float a[E], b[E], c2[E], d2[E];
-                gqtc::tmem_ld<E>(t_ahi + n0, a);
-                gqtc::tmem_ld<E>(t_ahi + N + n0, b);
-                gqtc::tmem_ld<E>(t_alo + n0, c2);
-                gqtc::tmem_ld<E>(t_alo + N + n0, d2);
+                float a[2 * E], b[2 * E];
+                gqtc::tmem_ld<2 * E>(t_ahi + 2 * n0, a);
+                gqtc::tmem_ld<2 * E>(t_alo + 2 * n0, b);
                 gqtc::tmem_wait_ld();
 #pragma unroll
-                for (int e = 0; e < E; ++e) {
-                    ur[e] = a[e] + c2[e];
-                    ui[e] = b[e] + d2[e];
-                }
+                for (int e = 0; e < E; ++e)
+                    U[e] = f2_add(make_float2(a[2 * e], a[2 * e + 1]), make_float2(b[2 * e], b[2 * e + 1]));
             }
             if constexpr (T::NGM < MM::NG) {  // diagonal terms in the epilogue: K += (sum_g c_g v_g[n]) u[n][j]
 #pragma unroll
                 for (int e = 0; e < E; ++e) {
-                    Cx<float> dv = {0.f, 0.f};
-#pragma unroll
-                    for (int g = 0; g < MM::NG; ++g) {
-                        const Cx<float> vg = ldc(MM::diag(g), n0 + e);
-                        const float cg = cs[(v * P + p) * NC + MM::ND + g];
-                        dv.re = fmaf(cg, vg.re, dv.re);
-                        dv.im = fmaf(cg, vg.im, dv.im);
-                    }
-                    Kr[e] = fmaf(dv.re, ur[e], fmaf(-dv.im, ui[e], Kr[e]));
-                    Ki[e] = fmaf(dv.re, ui[e], fmaf(dv.im, ur[e], Ki[e]));
+                    const Cx<float> dv = dvs[p * N + n0 + e];
+                    // Re K += dv.re ur - dv.im ui, Im K += dv.re ui + dv.im ur (the dv.im products first)
+                    W[e] = f2_fma(make_float2(dv.im, -dv.im), U[e], W[e]);
+                    W[e] = f2_fma(make_float2(dv.re, dv.re), make_float2(U[e].y, U[e].x), W[e]);
                 }
             }
         }  // !failed
@@ -458,11 +489,12 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
                 const uint32_t ka = gqtc::cluster_peer_u32(kbuf, peer) + (uint32_t)kidx * 8u;
                 const uint32_t kb = gqtc::cluster_peer_u32(kbar, peer);
 #pragma unroll
-                for (int e = 0; e < E; e += 2) gqtc::st_async_v4(ka + 8u * e, Kr[e], Ki[e], Kr[e + 1], Ki[e + 1], kb);
+                for (int e = 0; e < E; e += 2)
+                    gqtc::st_async_v4(ka + 8u * e, W[e].x, W[e].y, W[e + 1].x, W[e + 1].y, kb);
             } else {
                 float4* const kb = reinterpret_cast<float4*>(kbuf + kidx);
 #pragma unroll
-                for (int e = 0; e < E; e += 2) kb[e / 2] = make_float4(Kr[e], Ki[e], Kr[e + 1], Ki[e + 1]);
+                for (int e = 0; e < E; e += 2) kb[e / 2] = make_float4(W[e].x, W[e].y, W[e + 1].x, W[e + 1].y);
             }
         }
         if constexpr (T::CL > 1) {
@@ -472,13 +504,13 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
         }
 #pragma unroll
         for (int e = 0; e < E; ++e) {
-            const Cx<float> kt = kbuf[(p * NH + (n0 - nb + e)) * LDK + j];  // K[j][n], n = n0 + e
-            kre[e] = Ki[e] + kt.im;                             // -i (K[n][j] - conj(K[j][n]))
-            kim[e] = kt.re - Kr[e];
+            const float2 kt = kbuf[(p * NH + (n0 - nb + e)) * LDK + j];  // (Im, Re) of K[j][n], n = n0 + e
+            // -i (K[n][j] - conj(K[j][n])) = (Im K[n][j] + Im K[j][n], Re K[j][n] - Re K[n][j])
+            k[e] = f2_fma(W[e], make_float2(1.f, -1.f), kt);
         }
-        // jump terms of this thread: population rho_aa of the stage input into row e
-        float jre = 0.f, jim = 0.f;
-        for (int q = 0; q < jcount; ++q) {
+        // the other jump terms of this thread: population rho_aa of the stage input, or the element
+        // itself, into row e
+        for (int q = 0; q < (kJumpsEarly ? 0 : jcount); ++q) {
             const int idx = jl * MM::TCJ_MAX + q;
             const int rate = __ldg(MM::tcj_rate() + idx);
             Cx<float> w = ldc(MM::tcj_coef(), idx);
@@ -488,38 +520,32 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
                 w.im *= cr;
             }
             const int a = __ldg(MM::tcj_a() + idx);
-            if constexpr (MM::kJumpsOnDiagonal && !MM::kOwnTerms) {
-                const float x = rdiag[slot * P * N + p * N + a];
-                jre = fmaf(w.re, x, jre);
-                jim = fmaf(w.im, x, jim);
-            } else {
-                const int e = __ldg(MM::tcj_e() + idx);
-                const float x = (a >= 0) ? rdiag[slot * P * N + p * N + a] : 0.f;
+            const int e = __ldg(MM::tcj_e() + idx);
+            const float x = (a >= 0) ? rdiag[slot * P * N + p * N + a] : 0.f;
 #pragma unroll
-                for (int ee = 0; ee < E; ++ee)
-                    if (ee == e) {
-                        Cx<float> src = {x, 0.f};  // a population, or the element itself (a < 0)
-                        if constexpr (MM::kOwnTerms) {
-                            if (a < 0) src = {ur[ee], ui[ee]};
-                        }
-                        kre[ee] = fmaf(w.re, src.re, fmaf(-w.im, src.im, kre[ee]));
-                        kim[ee] = fmaf(w.re, src.im, fmaf(w.im, src.re, kim[ee]));
+            for (int ee = 0; ee < E; ++ee)
+                if (ee == e) {
+                    float2 src = make_float2(x, 0.f);  // a population, or the element itself (a < 0)
+                    if constexpr (MM::kOwnTerms) {
+                        if (a < 0) src = U[ee];
                     }
-            }
+                    // Re k += w.re src.re - w.im src.im, Im k += w.re src.im + w.im src.re (w.im first)
+                    k[ee] = f2_fma(make_float2(-w.im, w.im), make_float2(src.y, src.x), k[ee]);
+                    k[ee] = f2_fma(make_float2(w.re, w.re), src, k[ee]);
+                }
         }
         if constexpr (MM::kJumpsOnDiagonal) {
+            const float2 jv = make_float2(jre, jim);
 #pragma unroll
             for (int e = 0; e < E; ++e)
-                if (n0 + e == j) {
-                    kre[e] += jre;
-                    kim[e] += jim;
-                }
+                if (n0 + e == j) k[e] = f2_add(k[e], jv);
         }
         return true;
     };
 
     const float h = (float)dt, h2 = (float)dt2d;
     const Coef<float> h6 = Coef<float>::make(dt / 6.0);
+    const float2 h6_hi = make_float2(h6.hi, h6.hi), h6_lo = make_float2(h6.lo, h6.lo);
     double osum_re = 0.0, osum_im = 0.0;
     // Sum of (re, im) over the threads of point p, valid in its lead thread (of cluster rank 0): over
     // the point's columns in a warp (lanes p*N .. of at most 32), then over the row blocks and warps
@@ -569,7 +595,7 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             const Cx<double> o = ldc(MM::obs_t(), (n0 + e) * N + j);
-            const double xr = (double)yre[e], xi = (double)yim[e];
+            const double xr = (double)y[e].x, xi = (double)y[e].y;
             osum_re = fma(o.re, xr, fma(-o.im, xi, osum_re));
             osum_im = fma(o.re, xi, fma(o.im, xr, osum_im));
         }
@@ -580,18 +606,18 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
     // roundings of gqfixed::RK4, whose coefficients come from the table (block step / KB). The next
     // block's table is filled during the MMA of stage 1 of a block's last step.
     {
-        float kre[E], kim[E];
+        float2 k[E];
 #pragma unroll
-        for (int e = 0; e < E; ++e) kre[e] = kim[e] = 0.f;
+        for (int e = 0; e < E; ++e) k[e] = make_float2(0.f, 0.f);
         fill_table(0);
-        write_stage(0.f, kre, kim, 0);
+        write_stage(0.f, k, 0);
         const int total = 4 * d.num_steps;
         for (int it = 0; it < total; ++it) {
             const int step = it >> 2, s = it & 3;
             const int sb = step % T::KB;
             const int ver = ((step / T::KB) & 1) * T::TS + 3 * sb + (s == 0 ? 0 : (s == 3 ? 2 : 1));
             const int fill = (s == 1 && sb == T::KB - 1) ? step / T::KB + 1 : -1;
-            if (!eval(kre, kim, it & 1, ver, fill)) {  // (a single CTA only)
+            if (!eval(k, it & 1, ver, fill)) {  // (a single CTA only)
                 failed = true;
                 mma_lost = true;
                 break;
@@ -599,11 +625,9 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
             const int nslot = (it + 1) & 1;
             if (s == 3) {
 #pragma unroll
-                for (int e = 0; e < E; ++e) {
-                    are[e] += kre[e];
-                    aim[e] += kim[e];
-                    F::accumulate(yre[e], cre[e], are[e], h6);
-                    F::accumulate(yim[e], cim[e], aim[e], h6);
+                for (int e = 0; e < E; ++e) {  // FormFP32::accumulate on both parts
+                    acc[e] = f2_add(acc[e], k[e]);
+                    gq::f2_kahan(y[e], cn[e], acc[e], h6_hi, h6_lo);
                 }
                 if (OUT == GQIS_OUT_MEAN && step >= d.warmup_steps) observe();
                 if constexpr (TRACE == GQIS_TRACE_OBSERVABLE) {
@@ -626,23 +650,17 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
                 }
                 if (step + 1 == d.num_steps) break;
 #pragma unroll
-                for (int e = 0; e < E; ++e) kre[e] = kim[e] = 0.f;
-                write_stage(0.f, kre, kim, nslot);  // input of the next step's k1 (same time)
+                for (int e = 0; e < E; ++e) k[e] = make_float2(0.f, 0.f);
+                write_stage(0.f, k, nslot);  // input of the next step's k1 (same time)
             } else {
                 if (s == 0) {
 #pragma unroll
-                    for (int e = 0; e < E; ++e) {
-                        are[e] = kre[e];
-                        aim[e] = kim[e];
-                    }
+                    for (int e = 0; e < E; ++e) acc[e] = k[e];
                 } else {
 #pragma unroll
-                    for (int e = 0; e < E; ++e) {
-                        are[e] = fmaf(2.f, kre[e], are[e]);
-                        aim[e] = fmaf(2.f, kim[e], aim[e]);
-                    }
+                    for (int e = 0; e < E; ++e) acc[e] = f2_fma(make_float2(2.f, 2.f), k[e], acc[e]);
                 }
-                write_stage(s == 2 ? h : h2, kre, kim, nslot);
+                write_stage(s == 2 ? h : h2, k, nslot);
             }
         }
     }
@@ -667,11 +685,11 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
             for (int e = 0; e < E; ++e) {
                 const int n = n0 + e;
                 if (n == j && n < NO - 1) {
-                    dst[n] = yre[e];
+                    dst[n] = y[e].x;
                 } else if (n < j && j < NO) {
                     const int slot = NO - 1 + 2 * (n * NO - (n * (n + 1)) / 2 + (j - n - 1));
-                    dst[slot] = yre[e];
-                    dst[slot + 1] = yim[e];
+                    dst[slot] = y[e].x;
+                    dst[slot + 1] = y[e].y;
                 }
             }
         }

@@ -13,22 +13,9 @@
 #pragma once
 
 #include "gqis_common.cuh"
+#include "gqis_f32x2.cuh"
 
 namespace gq {
-
-__device__ __forceinline__ float2 f2_fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-__device__ __forceinline__ float2 f2_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 f2_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ float2 f2_sub(float2 a, float2 b) {
-    unsigned long long A = *reinterpret_cast<unsigned long long*>(&a);
-    unsigned long long B = *reinterpret_cast<unsigned long long*>(&b);
-    unsigned long long D;
-    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(D) : "l"(A), "l"(B));
-    return *reinterpret_cast<float2*>(&D);
-}
-// Sign flip of both lanes. Literal coefficients fold at compile time; a runtime operand becomes an
-// operand of the consuming packed instruction.
-__device__ __forceinline__ float2 f2_neg(float2 a) { return make_float2(-a.x, -a.y); }
 
 struct m2;
 
@@ -138,14 +125,10 @@ struct FormFP32x2 {
     using scalar_form = FormFP32;
     static constexpr int id = GQIS_FORM_FP32;
 
-    // Compensated y += h*a per lane with the correction kept negated (cn = -c), so every step is
-    // one packed instruction: v = a*h.hi + (a*h.lo + cn); s = y + v; cn = v - (s - y).
+    // Compensated y += h*a per lane with the correction kept negated (cn = -c): gq::f2_kahan.
     __device__ __forceinline__ static void accumulate(gq::f32x2& y, gq::f32x2& cn, const gq::f32x2& a,
                                                       float2 h_hi, float2 h_lo) {
-        const float2 v = gq::f2_fma(a.v, h_hi, gq::f2_fma(a.v, h_lo, cn.v));
-        const float2 s = gq::f2_add(y.v, v);
-        cn.v = gq::f2_sub(v, gq::f2_sub(s, y.v));
-        y.v = s;
+        gq::f2_kahan(y.v, cn.v, a.v, h_hi, h_lo);
     }
 
     // Compensated running sum per lane, flushed into FP64 every 256 terms (FormFP32::Sum per lane).

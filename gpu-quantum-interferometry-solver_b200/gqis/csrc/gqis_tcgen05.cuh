@@ -120,14 +120,38 @@ __device__ __forceinline__ void tmem_st4(uint32_t taddr, const float (&v)[4]) {
                  "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
                  "r"(__float_as_uint(v[3])));
 }
-// E consecutive columns (E = 4 or 8)
-template <int E>
-__device__ __forceinline__ void tmem_ld(uint32_t taddr, float (&v)[E]) {
-    if constexpr (E == 8) tmem_ld8(taddr, v); else tmem_ld4(taddr, v);
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
-template <int E>
-__device__ __forceinline__ void tmem_st(uint32_t taddr, const float (&v)[E]) {
-    if constexpr (E == 8) tmem_st8(taddr, v); else tmem_st4(taddr, v);
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float (&v)[16]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+        "%14, %15, %16};" ::"r"(taddr),
+        "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+        "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+        "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])), "r"(__float_as_uint(v[8])),
+        "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
+        "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])),
+        "r"(__float_as_uint(v[15])));
+}
+// C consecutive columns (C = 4, 8 or 16)
+template <int C>
+__device__ __forceinline__ void tmem_ld(uint32_t taddr, float (&v)[C]) {
+    static_assert(C == 4 || C == 8 || C == 16, "columns per tensor-memory load");
+    if constexpr (C == 16) tmem_ld16(taddr, v); else if constexpr (C == 8) tmem_ld8(taddr, v); else tmem_ld4(taddr, v);
+}
+template <int C>
+__device__ __forceinline__ void tmem_st(uint32_t taddr, const float (&v)[C]) {
+    static_assert(C == 4 || C == 8 || C == 16, "columns per tensor-memory store");
+    if constexpr (C == 16) tmem_st16(taddr, v); else if constexpr (C == 8) tmem_st8(taddr, v); else tmem_st4(taddr, v);
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }

@@ -548,7 +548,8 @@ def tensor_core_shape(mm: MatrixModel):
     cs = 2 * 24 * P * nc * 4  # coefficient table: 2 buffers x 3 stage times x 8 steps
     cg = Np // 32 if Np > 32 else 1
     off_red = -(-(2 * b + k + x + rd + cs) // 8) * 8
-    needed = off_red + 2 * H * cg * P * 8 + 2 * P * 8 + 64
+    dv = 0 if diag_in_mma(mm) or mm.num_diag == 0 else P * Np * 8  # the epilogue's diagonal coefficients
+    needed = off_red + 2 * H * cg * P * 8 + 2 * P * 8 + dv + 64
     return cl, nh, nmma, needed
 
 
