@@ -5,15 +5,15 @@
 // (N = padded dimension 8, 16, 32 or 64) is one M = 128 MMA:
 //
 //   row r = p*N + j  (point p of the tile, column j of its rho)  = tensor-memory lane r
-//   A[r][k]   = Re rho_p[m][j] (k = 2m),  Im rho_p[m][j] (k = 2m + 1)     (tensor memory)
+//   A[r][k]   = Re rho_p[m][j] (k = 2m),  Im rho_p[m][j] (k = 2m + 1)     (tensor memory, column m)
 //   B[k][col] = real embedding of T_q^T for the operator terms           (shared memory)
 //               T_0 = Heff0, T_q = M_q (dense, q = 1..ND), T_{ND+g} = diag(v_g) (g = 1..NG)
 //               col = 2 NH q + 2 (n - nb) + c, c = 0 (Im) / 1 (Re)
 //   D[r][col] = Im/Re (T_q rho_p)[n][j]                                    (tensor memory)
 //
-// Real and imaginary parts sit in adjacent columns, so one 32x32b load or store moves a thread's E
-// complex elements as (Im, Re) or (Re, Im) register pairs, on which the epilogue computes in packed
-// FP32 (one f32x2 instruction per complex element; each lane rounds as the scalar instruction).
+// Real and imaginary parts sit in adjacent D columns (and in one A column as two FP16), so one 32x32b
+// load or store moves a thread's E complex elements, on which the epilogue computes in packed FP32
+// (one f32x2 instruction per complex element; each lane rounds as the scalar instruction).
 //
 // Up to N = 32 one CTA holds the tile (NH = N rows n of every column, nb = 0). At N = 64 the
 // tile's state does not fit one SM's registers, so a cluster of CL = 2 CTAs shares it: CTA c owns
@@ -27,9 +27,12 @@
 // One MMA chain gives every point's T_q rho at once; the epilogue forms K = sum_q c_q(t) T_q rho
 // with the point's FP64-evaluated coefficients (c_0 = 1), -i (K - K^dag) through a transposed
 // read of K in shared memory, the jump terms, and the RK4 combination, and writes the next stage
-// input back into A. Operands are split TF32 (x = hi + lo, both TF32), three MMAs per K step
-// (hi*hi + hi*lo + lo*hi) with FP32 accumulation; the state is FP32 with the FP32 form's
-// compensated update, time and coefficients FP64, the mean of <O> FP64.
+// input back into A. Operands are split FP16 (x = hi + lo, both FP16, 22 significant bits as a split
+// TF32 pair), scaled by powers of two (A by 2^12, each operator term so that its largest entry is in
+// [2^12, 2^13)) that the epilogue undoes exactly; kind::f16 MMAs (K = 16, twice the K of kind::tf32 per
+// instruction at the same cycles), three per K step (hi*hi + hi*lo + lo*hi) with FP32 accumulation.
+// The state is FP32 with the FP32 form's compensated update, time and coefficients FP64, the mean of
+// <O> FP64.
 //
 // Thread t: lane r = t % 128 (warp quadrant r / 32), rows n0 = nb + E (t / 128) .. n0 + E - 1 of column j
 // (E = 8 rows per thread; the emitter may choose 4).
@@ -47,6 +50,8 @@
 // the loop, so its partner never waits in vain; the two tell each other at one cluster barrier after
 // the loop, and both write NaN. A CTA whose exchange wait gives up stops waiting altogether.
 #pragma once
+
+#include <cuda_fp16.h>
 
 #include <type_traits>
 
@@ -91,19 +96,21 @@ struct TcShape {
     static constexpr int NT = 1 + MM::ND + NGM;      // operator terms in B
     static constexpr int NMMA = 2 * NH * NT;  // B / D columns
     static constexpr int KDIM = 2 * N;        // real-embedded inner dimension
-    static constexpr int KCH = KDIM / 8;      // MMA K steps of 8 TF32
+    static constexpr int KCH = KDIM / 16;     // MMA K steps of 16 FP16
     static constexpr int NC = MM::NCOEF > 0 ? MM::NCOEF : 1;
     static constexpr int CG = N > 32 ? N / 32 : 1;  // warps spanned by one column set (point sums)
     static constexpr int KB = 8;              // steps per block of the coefficient table
     static constexpr int TS = 3 * KB;         // table slots per block: start, midpoint and end of each step
-    static constexpr int COL_D = 0, COL_AHI = NMMA, COL_ALO = NMMA + KDIM;
-    static constexpr int COLS_USED = NMMA + 2 * KDIM;
+    // A: one 32-bit column per row m of the stage input, (Re, Im) as two FP16 (K elements 2m, 2m + 1)
+    static constexpr int COL_D = 0, COL_AHI = NMMA, COL_ALO = NMMA + N;
+    static constexpr int COLS_USED = NMMA + 2 * N;
+    static constexpr int A_SCALE_EXP = 12;  // A = 2^12 u: |u| <= 16 stays below the FP16 maximum
     static constexpr uint32_t KSTEP_BYTES = 2u * NMMA * 32u;  // B of one K step: NMMA hi rows, then NMMA lo rows
     static constexpr int TMEM_COLS = tmem_alloc_cols(COLS_USED);
     static constexpr int LDK = N + 2;         // padded column stride of the K buffer (16-byte rows, no conflicts)
     static_assert(2 * E <= 16, "one 32x32b.x16 tensor-memory access per operand pair block");
     // shared memory layout (bytes)
-    static constexpr size_t B_BYTES = (size_t)NMMA * KDIM * 4;  // one of the two TF32 parts
+    static constexpr size_t B_BYTES = (size_t)NMMA * KDIM * 2;  // one of the two FP16 parts
     static constexpr size_t OFF_B = 0;
     static constexpr size_t OFF_K = 2 * B_BYTES;
     static constexpr size_t K_BYTES = (size_t)P * NH * LDK * 8;  // K[j][n] for the CTA's rows n, every j
@@ -119,7 +126,7 @@ struct TcShape {
     static constexpr size_t OFF_DV = OFF_RED + RED_BYTES;       // [P][N] sum_g c_g v_g[n] of the stage
     static constexpr size_t DV_BYTES = (NGM < MM::NG) ? (size_t)P * N * 8 : 0;
     static constexpr size_t OFF_MISC = OFF_DV + DV_BYTES;       // mbarriers, tensor-memory slot, failure flag
-    static constexpr size_t NEEDED = OFF_MISC + 64;
+    static constexpr size_t NEEDED = OFF_MISC + 128;  // + the terms' largest B entries (bits), at + 64
     // At most 512 / TMEM_COLS CTAs can hold tensor memory on one SM: pad the shared memory so that
     // no more CTAs fit (228 KB per SM, 1 KB reserved per CTA) and no allocation ever waits.
     static constexpr int MAX_CTAS = 512 / TMEM_COLS;
@@ -132,21 +139,32 @@ struct TcShape {
     static_assert(COLS_USED <= 512, "tensor memory columns");
     static_assert(SMEM <= 232448, "shared memory per CTA");
     static_assert(MIN_CTAS >= 1, "threads");
+    static_assert(NT <= 16, "operator terms (64 bytes of maxima)");
 };
 
-// Byte offset of B element (col, k) of TF32 part `part` (0 hi, 1 lo) in the K-major no-swizzle layout:
-// per K step of 8 the hi rows, then the lo rows, in groups of 8 (256 bytes: two 8 x 16-byte core
+// Byte offset of B element (col, k) of FP16 part `part` (0 hi, 1 lo) in the K-major no-swizzle layout:
+// per K step of 16 the hi rows, then the lo rows, in groups of 8 (256 bytes: two 8 x 16-byte core
 // matrices for the K halves).
 template <class T>
 __device__ __forceinline__ uint32_t b_offset(int col, int k, int part) {
-    return (uint32_t)((k >> 3) * T::KSTEP_BYTES + part * (T::NMMA * 32) + (col >> 3) * 256 + ((k & 7) >> 2) * 128 +
-                      (col & 7) * 16 + (k & 3) * 4);
+    return (uint32_t)((k >> 4) * T::KSTEP_BYTES + part * (T::NMMA * 32) + (col >> 3) * 256 + ((k & 15) >> 3) * 128 +
+                      (col & 7) * 16 + (k & 7) * 2);
 }
 
-// TF32 rounding (nearest, ties away from zero) of a finite FP32 number with integer operations:
-// add half a unit of the 10-bit mantissa's last place to the magnitude, clear the 13 dropped bits.
-__device__ __forceinline__ float tf32_round(float x) {
-    return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
+// Split FP16 of a scaled value x (|x| < 65504): hi = x rounded to FP16, lo = the exact remainder rounded
+// to FP16, both packed as one 32-bit word per lane pair; hi + lo keeps 22 significant bits (as a split
+// TF32 pair) down to |x| ~ 2^-3, and an absolute 2^-25 below.
+__device__ __forceinline__ void split_f16(float2 x, uint32_t& hi, uint32_t& lo) {
+    const __half2 h = __float22half2_rn(x);
+    const __half2 l = __float22half2_rn(f2_sub(x, __half22float2(h)));
+    hi = *reinterpret_cast<const uint32_t*>(&h);
+    lo = *reinterpret_cast<const uint32_t*>(&l);
+}
+// (hi + lo) of a split pair, unscaled by 2^-A_SCALE_EXP
+__device__ __forceinline__ float2 join_f16(uint32_t hi, uint32_t lo, float unscale) {
+    const float2 h = __half22float2(*reinterpret_cast<const __half2*>(&hi));
+    const float2 l = __half22float2(*reinterpret_cast<const __half2*>(&lo));
+    return gq::f2_mul(f2_add(h, l), make_float2(unscale, unscale));
 }
 
 template <class MM, int OUT, int TRACE>
@@ -155,7 +173,6 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
     constexpr int N = T::N, P = T::P, E = T::E, LDK = T::LDK, NO = MM::NO, NC = T::NC, NH = T::NH, H = T::H;
     static_assert(std::is_same<typename MM::real, float>::value, "tensor-core form uses FP32 model data");
     extern __shared__ __align__(1024) unsigned char gq_smem[];
-    float* const bsm = reinterpret_cast<float*>(gq_smem + T::OFF_B);
     float2* const kbuf = reinterpret_cast<float2*>(gq_smem + T::OFF_K);  // (Im, Re) of K[n][j]
     float2* const xbuf = reinterpret_cast<float2*>(gq_smem + T::OFF_X);
     float* const rdiag = reinterpret_cast<float*>(gq_smem + T::OFF_RD);
@@ -184,9 +201,9 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
     const bool active = local < d.point_count;
     const int64_t lp = active ? local : d.point_count - 1;  // idle rows integrate a copy of the last point
 
-    // ---- B = split-TF32 real embedding of the operator terms; mbarrier; tensor memory
-    for (int e = tid; e < T::NMMA * T::KDIM; e += T::THREADS) {
-        const int col = e / T::KDIM, k = e % T::KDIM;
+    // ---- B = split-FP16 real embedding of the operator terms, each term scaled by a power of two that
+    // puts its largest entry in [2^12, 2^13); mbarrier; tensor memory
+    auto b_entry = [&](int col, int k) -> float {
         const int q = col / (2 * NH), n = nb + (col % (2 * NH)) / 2;
         const bool re_out = (col & 1) != 0;  // output columns (Im, Re) of row n
         const int m = k >> 1;
@@ -202,12 +219,36 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
             ti = (n == m) ? __ldg(v + 2 * n + 1) : 0.f;
         }
         // Re out = sum Tr Re rho - Ti Im rho; Im out = sum Ti Re rho + Tr Im rho
-        const float val = re_out ? (imag_in ? -ti : tr) : (imag_in ? tr : ti);
-        const float hi = tf32_round(val);
-        const float lo = tf32_round(val - hi);
-        bsm[b_offset<T>(col, k, 0) >> 2] = hi;
-        bsm[b_offset<T>(col, k, 1) >> 2] = lo;
+        return re_out ? (imag_in ? -ti : tr) : (imag_in ? tr : ti);
+    };
+    uint32_t* const bmax = reinterpret_cast<uint32_t*>(gq_smem + T::OFF_MISC + 64);  // largest |entry| of
+    // each term (FP32 bits: non-negative floats order as unsigned integers)
+    if (tid < T::NT) bmax[tid] = 0u;
+    __syncthreads();
+    for (int e = tid; e < T::NMMA * T::KDIM; e += T::THREADS) {
+        const int col = e / T::KDIM;
+        atomicMax(&bmax[col / (2 * NH)], __float_as_uint(fabsf(b_entry(col, e % T::KDIM))));
     }
+    __syncthreads();
+    // 2^-(A scale + term scale): D_q back to the units of T_q rho (exact: powers of two)
+    auto term_exp = [&](int q) -> int {
+        const uint32_t bits = bmax[q];
+        if (bits == 0u) return 0;
+        const int ex = (int)((bits >> 23) & 0xFFu) - 127;  // floor(log2 max) of a normal number
+        return min(max(12 - ex, -24), 40);
+    };
+    __half* const bsm = reinterpret_cast<__half*>(gq_smem + T::OFF_B);
+    for (int e = tid; e < T::NMMA * T::KDIM; e += T::THREADS) {
+        const int col = e / T::KDIM, k = e % T::KDIM;
+        const float val = ldexpf(b_entry(col, k), term_exp(col / (2 * NH)));
+        const __half hi = __float2half_rn(val);
+        const __half lo = __float2half_rn(val - __half2float(hi));
+        bsm[b_offset<T>(col, k, 0) >> 1] = hi;
+        bsm[b_offset<T>(col, k, 1) >> 1] = lo;
+    }
+    float unscale[T::NT];
+#pragma unroll
+    for (int q = 0; q < T::NT; ++q) unscale[q] = ldexpf(1.f, -(T::A_SCALE_EXP + term_exp(q)));
     gqtc::fence_proxy_async_smem();
     if (tid == 0) {
         gqtc::mbar_init(bar, 1);
@@ -232,7 +273,7 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
     const uint32_t t_d = tbase + T::COL_D + lane_base;
     const uint32_t t_ahi = tbase + T::COL_AHI + lane_base;
     const uint32_t t_alo = tbase + T::COL_ALO + lane_base;
-    const uint32_t idesc = gqtc::idesc_tf32_m128(T::NMMA);
+    const uint32_t idesc = gqtc::idesc_f16_m128(T::NMMA);
     // B descriptor of K step 0; K step kc and the lo part are fixed offsets in its 14-bit address field
     // (shared-memory addresses stay below 2^18 bytes)
     const uint64_t bdesc0 = gqtc::smem_desc_kmajor(gqtc::smem_u32(bsm), 128, 256);
@@ -306,21 +347,21 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
         }
     };
 
-    // stage input u = y + s k -> A (hi / lo TF32 parts, (Re, Im) column pairs); populations ->
+    // stage input u = y + s k -> A (2^12 u as hi / lo FP16 parts, one column per row); populations ->
     // rdiag[slot]; in a cluster also into the partner's exchange buffer (its rows of A are this CTA's rows)
+    const float2 a_scale = make_float2((float)(1 << T::A_SCALE_EXP), (float)(1 << T::A_SCALE_EXP));
+    const float a_unscale = 1.f / (float)(1 << T::A_SCALE_EXP);
     auto write_stage = [&](float s, const float2 (&k)[E], int slot) {
-        float hv[2 * E], lv[2 * E];
+        float hv[E], lv[E];
         const float2 s2 = make_float2(s, s);
         float2 prev = make_float2(0.f, 0.f);  // the previous row's stage input
 #pragma unroll
         for (int e = 0; e < E; ++e) {
             const float2 u = f2_fma(s2, k[e], y[e]);
-            const float2 hi = make_float2(tf32_round(u.x), tf32_round(u.y));
-            const float2 lo = f2_sub(u, hi);  // |lo| <= 2^-11 |u|; its TF32 read loses at most 2^-21 |u|
-            hv[2 * e] = hi.x;
-            hv[2 * e + 1] = hi.y;
-            lv[2 * e] = lo.x;
-            lv[2 * e + 1] = lo.y;
+            uint32_t hb, lb;
+            split_f16(gq::f2_mul(u, a_scale), hb, lb);
+            hv[e] = __uint_as_float(hb);
+            lv[e] = __uint_as_float(lb);
             if (n0 + e == j) rdiag[slot * P * N + p * N + j] = u.x;
             if constexpr (T::CL > 1) {  // rows e - 1, e as one 16-byte remote store
                 if (e & 1)
@@ -330,8 +371,8 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
             }
             prev = u;
         }
-        gqtc::tmem_st<2 * E>(t_ahi + 2 * n0, hv);
-        gqtc::tmem_st<2 * E>(t_alo + 2 * n0, lv);
+        gqtc::tmem_st<E>(t_ahi + n0, hv);
+        gqtc::tmem_st<E>(t_alo + n0, lv);
     };
 
     uint32_t phase = 0, xphase = 0, kphase = 0;
@@ -359,27 +400,23 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
             exchange_wait(xbar, xphase, (uint32_t)T::X_BYTES);  // the partner's half of the stage input
             const int mb = (crank ^ 1) * NH + hh * E;
             const float4* xs = reinterpret_cast<const float4*>(xbuf) + (p * H + hh) * (E / 2) * N + j;
-            float hv[2 * E], lv[2 * E];  // rows mb .. mb + E - 1 as (Re, Im) pairs
+            float hv[E], lv[E];  // rows mb .. mb + E - 1, split as in write_stage
 #pragma unroll
             for (int e2 = 0; e2 < E / 2; ++e2) {
                 const float4 u = xs[e2 * N];
                 const float2 u0 = make_float2(u.x, u.y), u1 = make_float2(u.z, u.w);
-                const float2 h0 = make_float2(tf32_round(u0.x), tf32_round(u0.y));
-                const float2 h1 = make_float2(tf32_round(u1.x), tf32_round(u1.y));
-                const float2 l0 = f2_sub(u0, h0), l1 = f2_sub(u1, h1);
-                hv[4 * e2] = h0.x;
-                hv[4 * e2 + 1] = h0.y;
-                hv[4 * e2 + 2] = h1.x;
-                hv[4 * e2 + 3] = h1.y;
-                lv[4 * e2] = l0.x;
-                lv[4 * e2 + 1] = l0.y;
-                lv[4 * e2 + 2] = l1.x;
-                lv[4 * e2 + 3] = l1.y;
+                uint32_t h0, l0, h1, l1;
+                split_f16(gq::f2_mul(u0, a_scale), h0, l0);
+                split_f16(gq::f2_mul(u1, a_scale), h1, l1);
+                hv[2 * e2] = __uint_as_float(h0);
+                hv[2 * e2 + 1] = __uint_as_float(h1);
+                lv[2 * e2] = __uint_as_float(l0);
+                lv[2 * e2 + 1] = __uint_as_float(l1);
                 if (mb + 2 * e2 == j) rdiag[slot * P * N + p * N + j] = u0.x;
                 if (mb + 2 * e2 + 1 == j) rdiag[slot * P * N + p * N + j] = u1.x;
             }
-            gqtc::tmem_st<2 * E>(t_ahi + 2 * mb, hv);
-            gqtc::tmem_st<2 * E>(t_alo + 2 * mb, lv);
+            gqtc::tmem_st<E>(t_ahi + mb, hv);
+            gqtc::tmem_st<E>(t_alo + mb, lv);
         }
         gqtc::tmem_wait_st();
         gqtc::fence_before_sync();
@@ -390,9 +427,10 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
             for (int kc = 0; kc < T::KCH; ++kc) {
                 const uint64_t dh = bdesc0 + (uint64_t)((kc * T::KSTEP_BYTES) >> 4);
                 const uint64_t dl = dh + (uint64_t)((T::NMMA * 32) >> 4);
-                gqtc::mma_tf32_ts(tbase + T::COL_D, tbase + T::COL_AHI + 8 * kc, dh, idesc, kc > 0 ? 1u : 0u);
-                gqtc::mma_tf32_ts(tbase + T::COL_D, tbase + T::COL_AHI + 8 * kc, dl, idesc, 1u);
-                gqtc::mma_tf32_ts(tbase + T::COL_D, tbase + T::COL_ALO + 8 * kc, dh, idesc, 1u);
+                // K step kc: rows m = 8 kc .. 8 kc + 7 of the stage input, 8 columns of A
+                gqtc::mma_f16_ts(tbase + T::COL_D, tbase + T::COL_AHI + 8 * kc, dh, idesc, kc > 0 ? 1u : 0u);
+                gqtc::mma_f16_ts(tbase + T::COL_D, tbase + T::COL_AHI + 8 * kc, dl, idesc, 1u);
+                gqtc::mma_f16_ts(tbase + T::COL_D, tbase + T::COL_ALO + 8 * kc, dh, idesc, 1u);
             }
             gqtc::mma_commit(bar);
         }
@@ -454,21 +492,21 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
                 float dq[2 * E];
                 gqtc::tmem_ld<2 * E>(t_d + 2 * (q * NH + (n0 - nb)), dq);
                 gqtc::tmem_wait_ld();
-                const float2 c2 = make_float2(cq[q], cq[q]);
+                const float cu = cq[q] * unscale[q];  // D_q is 2^(A scale + term scale) T_q u
+                const float2 c2 = make_float2(cu, cu);
 #pragma unroll
                 for (int e = 0; e < E; ++e) {
                     const float2 d2 = make_float2(dq[2 * e], dq[2 * e + 1]);
-                    W[e] = (q == 0) ? d2 : f2_fma(c2, d2, W[e]);
+                    W[e] = (q == 0) ? gq::f2_mul(c2, d2) : f2_fma(c2, d2, W[e]);
                 }
             }
             if constexpr (MM::kOwnTerms || (T::NGM < MM::NG)) {  // terms that need the stage input itself
-                float a[2 * E], b[2 * E];
-                gqtc::tmem_ld<2 * E>(t_ahi + 2 * n0, a);
-                gqtc::tmem_ld<2 * E>(t_alo + 2 * n0, b);
+                float a[E], b[E];
+                gqtc::tmem_ld<E>(t_ahi + n0, a);
+                gqtc::tmem_ld<E>(t_alo + n0, b);
                 gqtc::tmem_wait_ld();
 #pragma unroll
-                for (int e = 0; e < E; ++e)
-                    U[e] = f2_add(make_float2(a[2 * e], a[2 * e + 1]), make_float2(b[2 * e], b[2 * e + 1]));
+                for (int e = 0; e < E; ++e) U[e] = join_f16(__float_as_uint(a[e]), __float_as_uint(b[e]), a_unscale);
             }
             if constexpr (T::NGM < MM::NG) {  // diagonal terms in the epilogue: K += (sum_g c_g v_g[n]) u[n][j]
 #pragma unroll

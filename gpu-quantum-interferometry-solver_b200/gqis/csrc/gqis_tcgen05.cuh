@@ -1,7 +1,7 @@
 // gqis_tcgen05.cuh - thin wrappers of the sm_100a tensor-core (tcgen05), tensor-memory and
 // mbarrier instructions used by gqis_matrix_tc.cuh, written as inline PTX (PTX ISA 8.7+).
 //
-// Only the forms this engine needs: cta_group::1, kind::tf32 with A in tensor memory and B in
+// Only the forms this engine needs: cta_group::1, kind::tf32 and kind::f16 with A in tensor memory and B in
 // shared memory (K-major, no swizzle), 32x32b tensor-memory loads/stores, mbarrier waits that give
 // up after a bounded number of polls, and the cluster barrier / distributed-shared-memory mapping
 // of two-CTA clusters (plain stores; no TMA, no multicast).
@@ -70,6 +70,17 @@ __device__ __forceinline__ void mma_tf32_ts(uint32_t d_tmem, uint32_t a_tmem, ui
         "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, {%5, %5, %5, %5}, p;\n\t}"
         ::"r"(d_tmem), "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(no_lane_disabled));
 }
+// D[tmem] (+)= A[tmem] x B[smem descriptor], kind::f16 (FP16 operands, K = 16 per MMA: a 32-bit
+// tensor-memory column of A holds two consecutive K elements), FP32 accumulate
+__device__ __forceinline__ void mma_f16_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc, uint32_t idesc,
+                                           uint32_t accumulate) {
+    const uint32_t no_lane_disabled = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, {%5, %5, %5, %5}, p;\n\t}"
+        ::"r"(d_tmem), "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(no_lane_disabled));
+}
 // Arrive on `bar` once every MMA issued so far by this thread has completed.
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
@@ -81,6 +92,15 @@ __host__ __device__ constexpr uint32_t idesc_tf32_m128(uint32_t n) {
     return (1u << 4)               // D format F32
            | (2u << 7)             // A format TF32
            | (2u << 10)            // B format TF32
+           | ((n >> 3) << 17)      // N / 8
+           | ((128u >> 4) << 24);  // M / 16
+}
+
+// Instruction descriptor: kind::f16 with FP16 A and B, FP32 accumulator, K-major, M = 128, N = n.
+__host__ __device__ constexpr uint32_t idesc_f16_m128(uint32_t n) {
+    return (1u << 4)               // D format F32
+           | (0u << 7)             // A format F16
+           | (0u << 10)            // B format F16
            | ((n >> 3) << 17)      // N / 8
            | ((128u >> 4) << 24);  // M / 16
 }

@@ -541,7 +541,7 @@ def tensor_core_shape(mm: MatrixModel):
     nmma = 2 * nh * terms
     kdim = 2 * Np
     nc = max(1, len(mm.coef_exprs))
-    b = nmma * kdim * 4
+    b = nmma * kdim * 2  # one FP16 part of B
     k = P * nh * (Np + 2) * 8
     x = P * H * E * Np * 8 if cl > 1 else 0
     rd = 2 * P * Np * 4
@@ -549,7 +549,7 @@ def tensor_core_shape(mm: MatrixModel):
     cg = Np // 32 if Np > 32 else 1
     off_red = -(-(2 * b + k + x + rd + cs) // 8) * 8
     dv = 0 if diag_in_mma(mm) or mm.num_diag == 0 else P * Np * 8  # the epilogue's diagonal coefficients
-    needed = off_red + 2 * H * cg * P * 8 + 2 * P * 8 + dv + 64
+    needed = off_red + 2 * H * cg * P * 8 + 2 * P * 8 + dv + 128  # + mbarriers, flags, B-term maxima
     return cl, nh, nmma, needed
 
 
