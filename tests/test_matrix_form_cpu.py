@@ -132,7 +132,8 @@ def test_tensor_core_jump_lists_of_a_dephased_qubit():
 
 def test_tensor_core_shape_of_the_two_cta_kernel():
     """N = 64 splits each tile's rows over a cluster of two CTAs: half the B columns per CTA, and the
-    shared memory (B, transposed K, exchange buffer) must fit one CTA; more dense operators do not."""
+    shared memory (B in two FP16 parts, transposed K, exchange buffer) fits one CTA up to the widest
+    MMA (256 columns: three dense operators and a diagonal one); more operators exceed one MMA."""
     from types import SimpleNamespace
     import numpy as np
 
@@ -144,8 +145,10 @@ def test_tensor_core_shape_of_the_two_cta_kernel():
     assert matrix_form.tensor_core_blockers(fake(64, 1, 1), "fp32") == []
     assert matrix_form.tensor_core_shape(fake(32, 1, 1))[:3] == (1, 32, 128)  # diagonal in the epilogue
     assert matrix_form.tensor_core_shape(fake(16, 1, 1))[:3] == (1, 16, 96)   # diagonal on the MMA
-    blocked = matrix_form.tensor_core_blockers(fake(64, 2, 1), "fp32")
-    assert len(blocked) == 1 and "shared memory" in blocked[0]
+    assert matrix_form.tensor_core_blockers(fake(64, 3, 1), "fp32") == []  # 2 x 32 x 4 = 256 columns
+    cl, nh, nmma, smem = matrix_form.tensor_core_shape(fake(64, 3, 1))
+    assert nmma == 256 and smem <= matrix_form.SMEM_LIMIT
+    assert "exceed one MMA" in matrix_form.tensor_core_blockers(fake(64, 4, 1), "fp32")[0]
     assert matrix_form.tensor_core_blockers(fake(32, 3, 1), "fp32") == []  # 2 x 32 x 4 = 256 columns
     assert "exceed one MMA" in matrix_form.tensor_core_blockers(fake(32, 4, 1), "fp32")[0]
     assert "padded dimension 48" in matrix_form.tensor_core_blockers(fake(48, 1, 1), "fp32")[0]
