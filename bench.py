@@ -309,7 +309,7 @@ def run_ours(args):
         torch.cuda.empty_cache()
         sys.path.insert(0, str(ROOT / "oracle"))
         sampler = ClockSampler(local).start()
-        hpeaks = {"fp64": peaks["fp64"], "fp32": peaks["fp32"], "tf32_tensor": native.probe_tc_tf32_tflops()}
+        hpeaks = {"fp64": peaks["fp64"], "fp32": peaks["fp32"], "f16_tensor": native.probe_tc_f16_tflops()}
         t_sub = time.perf_counter()
         line["hilbert"] = {"workload": HILBERT_WORKLOAD.format(steps=2000), "l2": "flushed between timed launches",
                            "measured_peaks_tflops": hpeaks,
@@ -511,7 +511,7 @@ def hilbert_rows(torch, dims, hsteps, flush, peaks, *, tc_reps=3, fp64_reps=1, c
     """Config C4 per dimension N: the tensor-core FP32 form against the plain FP64 density-matrix
     form on the full 64 x 64 map (both timed), the FP64 form pinned to the FP64 NumPy oracle on 4
     points, and the tensor-core kernel's roofline by the algorithmic count (16 N^3 per product
-    pair, no split passes) and by the MMAs it issues (three split-TF32 passes)."""
+    pair, no split passes) and by the MMAs it issues (three split-FP16 passes)."""
     import numpy as np
     import lindblad_oracle
     from gqis import solver, workloads
@@ -534,8 +534,8 @@ def hilbert_rows(torch, dims, hsteps, flush, peaks, *, tc_reps=3, fp64_reps=1, c
                      "warmup_launches": warm, "algorithmic_tflops": algo}
             if rhs_form == "matrix_tc":
                 mma = frag["tensor_flops_per_point_step"] * points * hsteps / (ms / 1e3) / 1e12
-                entry.update(mma_tflops=mma, frac_mma_of_measured_tf32=mma / peaks["tf32_tensor"],
-                             frac_algorithmic_of_measured_tf32=algo / peaks["tf32_tensor"])
+                entry.update(mma_tflops=mma, frac_mma_of_measured_f16=mma / peaks["f16_tensor"],
+                             frac_algorithmic_of_measured_f16=algo / peaks["f16_tensor"])
             else:
                 entry["frac_algorithmic_of_measured_fma"] = algo / peaks[prec]
             row[f"{rhs_form}_{prec}"] = entry
@@ -565,7 +565,7 @@ def run_hilbert(args):
     sys.path.insert(0, str(ROOT / "oracle"))
     from gqis import native
     peaks = {"fp64": native.probe_fma_tflops(0), "fp32": native.probe_fma_tflops(1),
-             "tf32_tensor": native.probe_tc_tf32_tflops()}
+             "f16_tensor": native.probe_tc_f16_tflops()}
     dims = tuple(int(n) for n in args.dims.split(","))
     flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
     sampler = ClockSampler(0).start()
@@ -575,7 +575,7 @@ def run_hilbert(args):
     hk = "16" if "16" in rows else str(dims[0])
     head = rows[hk]["matrix_tc_fp32"]
     line = {
-        "metric": "points*steps/s (RK4 density-matrix sweep, N-level scaling model; tensor-core split-TF32 "
+        "metric": "points*steps/s (RK4 density-matrix sweep, N-level scaling model; tensor-core split-FP16 "
                   "form, N=16 headline)",
         "value": head["points_steps_per_s"], "unit": "points*steps/s", "n_gpus": 1,
         "steps": args.steps, "warmup": 1, "ms_per_step": head["ms"], "higher_is_better": True,
@@ -583,11 +583,11 @@ def run_hilbert(args):
         "config": {"workload": HILBERT_WORKLOAD.format(steps=args.hsteps), "dims": list(dims),
                    "l2": "flushed (256 MiB write) between timed launches"},
         "per_dimension": rows,
-        "roofline": {"bound": "tensor", "achieved": head["algorithmic_tflops"], "peak": peaks["tf32_tensor"],
-                     "unit": "TFLOP/s", "frac": head["frac_algorithmic_of_measured_tf32"], "traffic": None,
-                     "peak_source": "tcgen05 kind::tf32 probe (gqis_probe_tc_tf32), same run",
+        "roofline": {"bound": "tensor", "achieved": head["algorithmic_tflops"], "peak": peaks["f16_tensor"],
+                     "unit": "TFLOP/s", "frac": head["frac_algorithmic_of_measured_f16"], "traffic": None,
+                     "peak_source": "tcgen05 kind::f16 probe (gqis_probe_tc_f16), same run",
                      "kernel": f"matrix_tc_kernel N={hk}", "mma_tflops": head["mma_tflops"],
-                     "frac_mma": head["frac_mma_of_measured_tf32"]},
+                     "frac_mma": head["frac_mma_of_measured_f16"]},
         "measured_fma_peaks_tflops": peaks, "clocks": clocks,
     }
     print(json.dumps(line))

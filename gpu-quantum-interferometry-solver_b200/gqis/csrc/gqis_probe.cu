@@ -63,12 +63,14 @@ __global__ void __launch_bounds__(kBlock) fma32x2_kernel(int iters, float* out) 
     if (s == 123.456f) out[blockIdx.x] = s;
 }
 
-// ---- tcgen05 kind::tf32: one CTA per SM issues `iters` x 4 MMAs of M = 128, N = 256, K = 8 (A in
-// tensor memory, B in shared memory, as the density-matrix kernel does) back to back and waits once.
+// ---- tcgen05 kind::tf32 (KIND 0, K = 8) or kind::f16 (KIND 1, K = 16): one CTA per SM issues `iters` x 4
+// MMAs of M = 128, N = 256 (A in tensor memory, B in shared memory, as the density-matrix kernel does)
+// back to back and waits once. Both kinds read the same bytes per MMA (32 per row of A and of B).
 constexpr int kTcN = 256, kTcKSteps = 4;
 constexpr size_t kTcSmem = 120 * 1024;  // > half of the SM's shared memory: one CTA per SM
 
-__global__ void __launch_bounds__(128, 1) tc_tf32_kernel(int iters, float* out, int* status) {
+template <int KIND>
+__global__ void __launch_bounds__(128, 1) tc_mma_kernel(int iters, float* out, int* status) {
     extern __shared__ __align__(1024) unsigned char smem[];
     float* b = reinterpret_cast<float*>(smem);  // kTcKSteps x 256 rows x 8 TF32, K-major
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kTcKSteps * kTcN * 32);
@@ -97,13 +99,17 @@ __global__ void __launch_bounds__(128, 1) tc_tf32_kernel(int iters, float* out, 
     bool ok = true;
     if (tid == 0) {
         gqtc::fence_after_sync();
-        const uint32_t idesc = gqtc::idesc_tf32_m128(kTcN);
+        const uint32_t idesc = KIND == 0 ? gqtc::idesc_tf32_m128(kTcN) : gqtc::idesc_f16_m128(kTcN);
         const uint32_t baddr = gqtc::smem_u32(b);
         for (int it = 0; it < iters; ++it) {
 #pragma unroll
-            for (int kc = 0; kc < kTcKSteps; ++kc)
-                gqtc::mma_tf32_ts(tbase, tbase + kTcN + 8 * kc, gqtc::smem_desc_kmajor(baddr + kc * kTcN * 32, 128, 256),
-                                  idesc, (it | kc) ? 1u : 0u);
+            for (int kc = 0; kc < kTcKSteps; ++kc) {
+                const uint64_t bd = gqtc::smem_desc_kmajor(baddr + kc * kTcN * 32, 128, 256);
+                if constexpr (KIND == 0)
+                    gqtc::mma_tf32_ts(tbase, tbase + kTcN + 8 * kc, bd, idesc, (it | kc) ? 1u : 0u);
+                else
+                    gqtc::mma_f16_ts(tbase, tbase + kTcN + 8 * kc, bd, idesc, (it | kc) ? 1u : 0u);
+            }
         }
         gqtc::mma_commit(bar);
         ok = gqtc::mbar_wait_bounded(bar, 0, 1u << 26);
@@ -123,18 +129,15 @@ __global__ void __launch_bounds__(128, 1) tc_tf32_kernel(int iters, float* out, 
     }
 }
 
-}  // namespace
-
-extern "C" {
-
-// Measured dense TF32 tensor-core rate (best of `repeats` launches after a warm-up) in 1e12 flop/s.
-// Returns GQIS_ERR_CUDA if an MMA chain did not signal completion within its bounded wait.
-__attribute__((visibility("default"))) int gqis_probe_tc_tf32(int iters, int repeats, double* tflops) {
+// Measured dense tensor-core rate of kind KIND (best of `repeats` launches after a warm-up) in 1e12
+// flop/s. GQIS_ERR_CUDA if an MMA chain did not signal completion within its bounded wait.
+template <int KIND>
+int probe_tc(int iters, int repeats, double* tflops) {
     if (!tflops || iters < 1 || repeats < 1) return GQIS_ERR_INVALID;
     int dev = 0, sms = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return GQIS_ERR_CUDA;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return GQIS_ERR_CUDA;
-    if (cudaFuncSetAttribute(tc_tf32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem) != cudaSuccess)
+    if (cudaFuncSetAttribute(tc_mma_kernel<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem) != cudaSuccess)
         return GQIS_ERR_CUDA;
     void* out = nullptr;
     int* status = nullptr;
@@ -151,7 +154,7 @@ __attribute__((visibility("default"))) int gqis_probe_tc_tf32(int iters, int rep
     int rc = GQIS_OK;
     for (int r = 0; r <= repeats; ++r) {
         cudaEventRecord(e0);
-        tc_tf32_kernel<<<sms, 128, kTcSmem>>>(iters, (float*)out, status);
+        tc_mma_kernel<KIND><<<sms, 128, kTcSmem>>>(iters, (float*)out, status);
         cudaEventRecord(e1);
         if (cudaEventSynchronize(e1) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
             rc = GQIS_ERR_CUDA;
@@ -159,7 +162,7 @@ __attribute__((visibility("default"))) int gqis_probe_tc_tf32(int iters, int rep
         }
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, e0, e1);
-        const double flops = 2.0 * 128.0 * kTcN * 8.0 * kTcKSteps * (double)iters * sms;
+        const double flops = 2.0 * 128.0 * kTcN * (KIND == 0 ? 8.0 : 16.0) * kTcKSteps * (double)iters * sms;
         if (r > 0 && ms > 0.0f) best = fmax(best, flops / (ms * 1e-3) / 1e12);
     }
     int host_status = 0;
@@ -172,6 +175,17 @@ __attribute__((visibility("default"))) int gqis_probe_tc_tf32(int iters, int rep
     cudaFree(status);
     *tflops = best;
     return rc;
+}
+}  // namespace
+
+extern "C" {
+
+// Measured dense TF32 (kind::tf32) / FP16 (kind::f16) tensor-core rate in 1e12 flop/s.
+__attribute__((visibility("default"))) int gqis_probe_tc_tf32(int iters, int repeats, double* tflops) {
+    return probe_tc<0>(iters, repeats, tflops);
+}
+__attribute__((visibility("default"))) int gqis_probe_tc_f16(int iters, int repeats, double* tflops) {
+    return probe_tc<1>(iters, repeats, tflops);
 }
 
 

@@ -213,11 +213,5 @@ __device__ __forceinline__ void st_async_v4(uint32_t addr, float a, float b, flo
                  : "memory");
 }
 
-// Round to TF32 (nearest, ties away from zero); the result is an FP32 number with 10 mantissa bits.
-__device__ __forceinline__ float to_tf32(float x) {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return __uint_as_float(r);
-}
 
 }  // namespace gqtc

@@ -392,9 +392,12 @@ def tensor_core_jump_lists(mm: MatrixModel, rows_per_thread=8):
 
 def diag_in_mma(mm: MatrixModel):
     """Whether the tensor-core kernel multiplies the diagonal operator terms on the tensor cores
-    (one more MMA term per diagonal operator) or in its epilogue. Up to N = 16 the epilogue is
-    the longer part of a stage and the MMA has room; at N = 32 the MMA is the longer part."""
-    return mm.Np <= 16
+    (one more MMA term per diagonal operator) or in its epilogue: on the tensor cores wherever the MMA
+    is wide enough (2 x rows x terms <= 256 columns). With FP16 operands (K = 16 per MMA) that is the
+    faster side at every N: 4096 points x 2000 steps, N = 32 113 ms vs 130 ms with the diagonal terms
+    in the epilogue (which reads the stage input back from A), N = 64 1081 vs 1165 ms."""
+    rows = mm.Np // (2 if mm.Np >= TC_CLUSTER_FROM else 1)
+    return 2 * rows * (1 + mm.num_dense + mm.num_diag) <= 256
 
 
 # Rows of a column per thread of the tensor-core kernel, by padded dimension (4 or 8). Four rows double
@@ -632,7 +635,7 @@ def algorithmic_flops_per_point_step(mm: MatrixModel):
     complex multiply-add) plus the kernel's element-wise terms (coefficients, diagonal and jump
     terms, -i(K - K^dag)); per step 4 RHS, the RK4 stage arithmetic (26 per element) and <O>
     (8 per element). Uses the model's dimension N, not the padded tile, and counts neither the
-    padding nor the extra split-TF32 passes of the tensor-core kernel."""
+    padding nor the extra split-FP16 passes of the tensor-core kernel."""
     N = mm.N
     nn = N * N
     elementwise = 4 * mm.num_dense * nn + (8 * nn + 4 * mm.num_diag * N if mm.num_diag else 0)
@@ -642,7 +645,7 @@ def algorithmic_flops_per_point_step(mm: MatrixModel):
 
 def tensor_flops_per_point_step(mm: MatrixModel):
     """Tensor-pipe arithmetic of one RK4 step of one point in the tcgen05 kernel: per RHS the
-    point's N rows of D (2 N (1 + ND + NG) columns) over K = 2 N, three split-TF32 passes."""
+    point's N rows of D (2 N (1 + ND + NG) columns) over K = 2 N, three split-FP16 passes."""
     Np = mm.Np
     terms = 1 + mm.num_dense + (mm.num_diag if diag_in_mma(mm) else 0)
     return 4 * 3 * 2 * Np * (2 * Np * terms) * (2 * Np)

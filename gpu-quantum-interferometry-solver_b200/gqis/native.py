@@ -1,6 +1,6 @@
 """The package's fixed native libraries (built in-tree by nvcc for sm_100a).
 
-* ``libgqis_probe.so``  - FMA-pipe and TF32 tensor-core throughput probes (roofline denominators);
+* ``libgqis_probe.so``  - FMA-pipe and TF32 / FP16 tensor-core throughput probes (roofline denominators);
 * ``libgqis_render.so`` - phase-space rasteriser kernels (``gqis.render``);
 * ``libgqis_serve.so``  - native sweep server for C/C++ hosts (``include/gqis_serve.h``).
 
@@ -79,13 +79,24 @@ def probe_fma_tflops(kind, iters=4096, repeats=3):
     return out.value
 
 
+def _probe_tc(symbol, iters, repeats):
+    lib = load("gqis_probe")
+    fn = getattr(lib, symbol)
+    fn.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    fn.restype = ctypes.c_int
+    out = ctypes.c_double()
+    rc = fn(int(iters), int(repeats), ctypes.byref(out))
+    if rc != 0:
+        raise RuntimeError(f"{symbol} failed with status {rc}")
+    return out.value
+
+
 def probe_tc_tf32_tflops(iters=4096, repeats=3):
     """Measured dense TF32 tensor-core rate in TFLOP/s (tcgen05 kind::tf32, M=128, N=256, K=8)."""
-    lib = load("gqis_probe")
-    lib.gqis_probe_tc_tf32.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
-    lib.gqis_probe_tc_tf32.restype = ctypes.c_int
-    out = ctypes.c_double()
-    rc = lib.gqis_probe_tc_tf32(int(iters), int(repeats), ctypes.byref(out))
-    if rc != 0:
-        raise RuntimeError(f"gqis_probe_tc_tf32 failed with status {rc}")
-    return out.value
+    return _probe_tc("gqis_probe_tc_tf32", iters, repeats)
+
+
+def probe_tc_f16_tflops(iters=4096, repeats=3):
+    """Measured dense FP16 tensor-core rate in TFLOP/s (tcgen05 kind::f16, M=128, N=256, K=16), the
+    instruction of the density-matrix tensor-core kernel."""
+    return _probe_tc("gqis_probe_tc_f16", iters, repeats)

@@ -483,7 +483,7 @@ def _solve_symbolic_system(H, Drive, Col_Ops, mean_operator, tlist,
     ``rhs_form``: ``"reduced"`` (the reference's N*N-1 real equations), ``"matrix"`` (the
     density-matrix kernel of ``matrix_form`` on the CUDA cores; fixed-step RK4, outputs
     ``mean``/``final``/``final_rho`` and the observable time trace), ``"matrix_tc"`` (the same on the tensor
-    cores, split-TF32 operands with FP32 accumulation; FP32 form, padded N of 8, 16, 32 or 64) or
+    cores, split-FP16 operands with FP32 accumulation; FP32 form, padded N of 8, 16, 32 or 64) or
     ``"auto"`` (matrix from N = 8 on where it applies, on the tensor cores for FP32 sweeps the
     tensor-core kernel can run).
     """

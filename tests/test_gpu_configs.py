@@ -4,7 +4,7 @@ The other GPU tests pin each kernel on small grids; these run the Hilbert-space 
 (64 x 64 points, 2000 RK4 steps) and the adaptive Duffing sweep (1024 x 1024 points, t in
 [0, 500]) exactly as the benchmark does and check them at that size:
 
-* tensor-core density-matrix kernel (split-TF32 MMAs, FP32 state) against the plain FP64
+* tensor-core density-matrix kernel (split-FP16 MMAs, FP32 state) against the plain FP64
   density-matrix form on the whole 4096-point map, <= 1e-6 max-abs; the FP64 form itself against
   the NumPy FP64 oracle on 4 points, <= 1e-11;
 * Tsit5A against the reference's own generated tsit5a kernel for the same call, compiled for

@@ -8,7 +8,7 @@
 * final_rho in the reduced layout, and rho0_values read back from it (a run split in two
   equals the run in one piece);
 * rhs_form="auto" picks the matrix form from N = 8 on (tensor cores for FP32);
-* the tensor-core kernel (split-TF32 tcgen05 MMAs, FP32 accumulation and state) against the same
+* the tensor-core kernel (split-FP16 tcgen05 MMAs, FP32 accumulation and state) against the same
   oracle at N = 8, 16, 32: 5e-6 max-abs, and within 5e-6 of the CUDA-core FP32 form; final_rho
   through it as well. The grids leave the last tile of points partly empty.
 """

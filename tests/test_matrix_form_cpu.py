@@ -133,7 +133,8 @@ def test_tensor_core_jump_lists_of_a_dephased_qubit():
 def test_tensor_core_shape_of_the_two_cta_kernel():
     """N = 64 splits each tile's rows over a cluster of two CTAs: half the B columns per CTA, and the
     shared memory (B in two FP16 parts, transposed K, exchange buffer) fits one CTA up to the widest
-    MMA (256 columns: three dense operators and a diagonal one); more operators exceed one MMA."""
+    MMA (256 columns: three dense operators, the diagonal one then in the epilogue); more dense
+    operators exceed one MMA."""
     from types import SimpleNamespace
     import numpy as np
 
@@ -141,9 +142,10 @@ def test_tensor_core_shape_of_the_two_cta_kernel():
         return SimpleNamespace(Np=Np, num_dense=dense, num_diag=diag, coef_exprs=[0] * (dense + diag),
                                jumps=[], wjump=np.zeros((Np, Np)))
     cl, nh, nmma, smem = matrix_form.tensor_core_shape(fake(64, 1, 1))
-    assert (cl, nh, nmma) == (2, 32, 128) and smem <= matrix_form.SMEM_LIMIT
+    assert (cl, nh, nmma) == (2, 32, 192) and smem <= matrix_form.SMEM_LIMIT  # diagonal on the MMA
     assert matrix_form.tensor_core_blockers(fake(64, 1, 1), "fp32") == []
-    assert matrix_form.tensor_core_shape(fake(32, 1, 1))[:3] == (1, 32, 128)  # diagonal in the epilogue
+    assert matrix_form.tensor_core_shape(fake(32, 1, 1))[:3] == (1, 32, 192)  # diagonal on the MMA
+    assert matrix_form.tensor_core_shape(fake(32, 3, 1))[:3] == (1, 32, 256)  # 320 columns: in the epilogue
     assert matrix_form.tensor_core_shape(fake(16, 1, 1))[:3] == (1, 16, 96)   # diagonal on the MMA
     assert matrix_form.tensor_core_blockers(fake(64, 3, 1), "fp32") == []  # 2 x 32 x 4 = 256 columns
     cl, nh, nmma, smem = matrix_form.tensor_core_shape(fake(64, 3, 1))
