@@ -507,11 +507,12 @@ def run_two_level(args):
     return 0
 
 
-def hilbert_rows(torch, dims, hsteps, flush, peaks, *, tc_reps=3, fp64_reps=1, cuda_fp32=False):
+def hilbert_rows(torch, dims, hsteps, flush, peaks, *, tc_reps=3, fp64_reps=1, cuda_fp32=False, only=()):
     """Config C4 per dimension N: the tensor-core FP32 form against the plain FP64 density-matrix
     form on the full 64 x 64 map (both timed), the FP64 form pinned to the FP64 NumPy oracle on 4
     points, and the tensor-core kernel's roofline by the algorithmic count (16 N^3 per product
-    pair, no split passes) and by the MMAs it issues (three split-FP16 passes)."""
+    pair, no split passes) and by the MMAs it issues (three split-FP16 passes). ``only``: names of
+    the forms to run (e.g. "matrix_tc_fp32"); the comparisons with a form that did not run are left out."""
     import numpy as np
     import lindblad_oracle
     from gqis import solver, workloads
@@ -523,6 +524,8 @@ def hilbert_rows(torch, dims, hsteps, flush, peaks, *, tc_reps=3, fp64_reps=1, c
         forms = [("matrix_tc", "fp32", tc_reps, 1), ("matrix", "fp64", fp64_reps, 1 if N < 64 else 0)]
         if cuda_fp32:
             forms.append(("matrix", "fp32", tc_reps, 1))
+        if only:
+            forms = [f for f in forms if f"{f[0]}_{f[1]}" in only]
         row, maps = {}, {}
         for rhs_form, prec, reps, warm in forms:
             sweep = solver.prepare_sweep("mesolve_2D", *model, var_arrays=w["var_arrays"], precision=prec,
@@ -546,13 +549,14 @@ def hilbert_rows(torch, dims, hsteps, flush, peaks, *, tc_reps=3, fp64_reps=1, c
         sub = {eps: np.asarray(w["var_arrays"][eps])[idx[:2]], A: np.asarray(w["var_arrays"][A])[idx[2:]]}
         ref = lindblad_oracle.rk4_sweep(lindblad_oracle.from_workload(w, sub), w["tlist"]).reshape(-1)
         sel = (idx[:2][:, None] * 64 + idx[2:][None, :]).reshape(-1)
-        full64 = maps[("matrix", "fp64")]
+        full64 = maps.get(("matrix", "fp64"))
         for (rhs_form, prec), m in maps.items():
             got = m[sel, 0] + 1j * m[sel, 1]
             row[f"{rhs_form}_{prec}"]["max_abs_vs_fp64_oracle_4pts"] = float(np.max(np.abs(got - ref)))
-            if prec == "fp32":
+            if prec == "fp32" and full64 is not None:
                 row[f"{rhs_form}_{prec}"]["max_abs_vs_fp64_form_full_map"] = float(np.max(np.abs(m - full64)))
-        row["tensor_core_speedup_vs_fp64"] = row["matrix_fp64"]["ms"] / row["matrix_tc_fp32"]["ms"]
+        if "matrix_fp64" in row and "matrix_tc_fp32" in row:
+            row["tensor_core_speedup_vs_fp64"] = row["matrix_fp64"]["ms"] / row["matrix_tc_fp32"]["ms"]
         rows[str(N)] = row
     return rows
 
@@ -569,10 +573,14 @@ def run_hilbert(args):
     dims = tuple(int(n) for n in args.dims.split(","))
     flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
     sampler = ClockSampler(0).start()
+    only = tuple(f for f in args.forms.split(",") if f)
     rows = hilbert_rows(torch, dims, args.hsteps, flush, peaks, tc_reps=max(1, args.steps // 2),
-                        cuda_fp32=True)
+                        cuda_fp32=True, only=only)
     clocks = sampler.stop()
     hk = "16" if "16" in rows else str(dims[0])
+    if "matrix_tc_fp32" not in rows[hk]:
+        print(json.dumps({"per_dimension": rows, "measured_fma_peaks_tflops": peaks, "clocks": clocks}))
+        return 0
     head = rows[hk]["matrix_tc_fp32"]
     line = {
         "metric": "points*steps/s (RK4 density-matrix sweep, N-level scaling model; tensor-core split-FP16 "
