@@ -185,3 +185,27 @@ def test_dimension_40_runs_on_the_tensor_cores_padded_to_64():
     ref = _oracle(w, kwargs)
     assert float(np.max(np.abs(fp64 - ref))) <= 1e-11
     assert float(np.max(np.abs(tc - ref))) <= 2e-6
+
+
+@pytest.mark.gpu
+def test_tensor_core_split_fp16_keeps_entries_far_below_a_terms_largest():
+    """The split-FP16 operands are scaled per operator term by the term's largest entry: level energies
+    up to 45.5 share Heff0 with couplings of 2e-3 and decay terms of 5e-5 (below the smallest normal
+    FP16 number unscaled), and the drive operator holds 1 beside 3e-4. The decay terms move the driven
+    population (level 1) by more than 1e-4; the tensor-core form matches the FP64 form there to 2e-6,
+    and the population fed only by the small couplings (level 2) to 1% of its size."""
+    import gqis
+    from test_support_calls import wide_range_model
+
+    def run(level, tc, decay=True):
+        args, kwargs = wide_range_model(level, decay)
+        form = dict(precision="fp32", rhs_form="matrix_tc") if tc else dict(fp64=True, rhs_form="matrix")
+        return gqis.mesolve_2D(*args, **kwargs, **form)
+
+    ref1 = run(1, False)
+    assert np.max(np.abs(ref1)) > 0.05  # the resonant drive moves level 1
+    assert float(np.max(np.abs(ref1 - run(1, False, decay=False)))) > 1e-4  # the decay terms matter
+    assert float(np.max(np.abs(run(1, True) - ref1))) <= 2e-6
+    ref2 = run(2, False)
+    assert 1e-8 < float(np.max(np.abs(ref2))) < 1e-3  # fed by the small couplings only
+    assert float(np.max(np.abs(run(2, True) - ref2))) <= 1e-2 * float(np.max(np.abs(ref2)))

@@ -69,6 +69,7 @@ def matrix_calls():
     out.append(("mesolve_2D", args, dict(kwargs, fp64=True, rhs_form="matrix", output_mode="final_rho",
                                          rho0_values=rho0)))
     out += runtime_rate_calls()
+    out += wide_range_calls()
     args, kwargs = serving_model(8, 6)  # observable traces through the matrix kernels
     args = args[:4] + (np.linspace(0.0, 5.0, 101),)
     trace = dict(kwargs, return_time_trace=True, time_trace_every=7)
@@ -258,4 +259,42 @@ def known_answer_calls():
     out.append(("mesolve_2D",) + commuting_call("rk4", "mean"))
     out.append(("mesolve_2D",) + decay_call())
     out.append(("odesolve_2D",) + ode_call())
+    return out
+
+
+def wide_range_model(level, decay=True):
+    """(args, kwargs) of an 8-level model whose operator terms span many orders of magnitude: level
+    energies up to 45.5 with couplings of 2e-3 and decay terms of 5e-5 in Heff0, a drive operator of
+    1 beside 3e-4; resonant drive A cos(6.5 t); mean population of `level`; 7 x 6 (eps, A) grid,
+    2000 RK4 steps on [0, 20]."""
+    eps, A, Drive, t = sp.symbols("eps A Drive t", real=True)
+    N = 8
+    H0 = sp.zeros(N)
+    for k in range(N):
+        H0[k, k] = 6.5 * k
+    for k in range(N - 1):
+        H0[k, k + 1] = H0[k + 1, k] = 2e-3
+    X = sp.zeros(N)
+    X[0, 1] = X[1, 0] = 1
+    for k in range(1, N - 1):
+        X[k, k + 1] = X[k + 1, k] = 3e-4
+    H = H0 + eps * sp.diag(*range(N)) + Drive * X
+    col = []
+    for k in range(1, N) if decay else ():
+        L = sp.zeros(N)
+        L[k - 1, k] = sp.sqrt(1e-4)
+        col.append(L)
+    O = sp.zeros(N)
+    O[level, level] = 1
+    var = {eps: np.linspace(-0.05, 0.05, 7), A: np.linspace(0.2, 2.0, 6)}
+    return (H, A * sp.cos(6.5 * t), col, O, np.linspace(0.0, 20.0, 2001)), {"var_arrays": var}
+
+
+def wide_range_calls():
+    out = []
+    for level, decay in ((1, True), (1, False), (2, True)):
+        args, kwargs = wide_range_model(level, decay)
+        out.append(("mesolve_2D", args, dict(kwargs, fp64=True, rhs_form="matrix")))
+        if decay:
+            out.append(("mesolve_2D", args, dict(kwargs, precision="fp32", rhs_form="matrix_tc")))
     return out
