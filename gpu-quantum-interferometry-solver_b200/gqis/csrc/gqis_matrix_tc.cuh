@@ -36,8 +36,8 @@
 //
 // Thread t: lane r = t % 128 (warp quadrant r / 32), rows n0 = nb + E (t / 128) .. n0 + E - 1 of column j
 // (E = 8 rows per thread; the emitter may choose 4).
-// Diagonal operator terms go through the MMA (kDiagInMma, small N) or the epilogue (larger N,
-// where the MMA is the longer part of a stage). Coefficients are evaluated in FP64 for every point
+// Diagonal operator terms go through the MMA (kDiagInMma, wherever the MMA is wide enough) or the
+// epilogue (their per-point sums formed while the MMA runs). Coefficients are evaluated in FP64 for every point
 // and stage time of KB steps at once, spread over all threads while an MMA runs, into a
 // double-buffered table in shared memory. Jump terms come from per-thread
 // lists (the module's tcj_* tables) whose sources are populations rho_aa, shared through shared
