@@ -44,7 +44,8 @@
 // memory when the stage input is written, or the thread's own element (element-wise terms on
 // coherences, kOwnTerms); those and the diagonal terms done in the epilogue read the stage input
 // back from A (hi + lo).
-// One thread polls the MMA's mbarrier (bounded); the CTA meets it at a barrier. On give-up the
+// Every thread polls the MMA's mbarrier (bounded; in a cluster one thread, and the CTA meets it at a
+// barrier); a give-up is made uniform over the CTA at the next barrier. On give-up the
 // CTA writes NaN outputs, waits (bounded) for the MMA in flight, frees its tensor memory and returns.
 // A CTA of a cluster instead stops using the tensor cores but keeps exchanging (zeros) to the end of
 // the loop, so its partner never waits in vain; the two tell each other at one cluster barrier after
@@ -470,12 +471,12 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
                 dvs[idx] = dv;
             }
         }
-        // one thread polls the mbarrier; the others wait at the barrier instead of spinning
-        const bool ok = (tid != 0) || failed || gqtc::mbar_wait_bounded(bar, phase, kMaxPolls);
-        const bool bad = __syncthreads_or(!ok);  // MMA complete (or given up, uniformly over the CTA)
-        if constexpr (T::CL == 1) {
-            if (bad) return false;
-        }
+        // One CTA per tile: every thread waits for the MMA itself (bounded), so each warp starts its
+        // epilogue as soon as the MMA has completed; a give-up is made uniform over the warp at once (the
+        // tensor-memory loads below are warp-aligned) and over the CTA at the K barrier. In a cluster one
+        // thread polls and the CTA meets at a barrier.
+        const bool ok = (T::CL == 1 || tid == 0) ? (failed || gqtc::mbar_wait_bounded(bar, phase, kMaxPolls)) : true;
+        const bool bad = T::CL == 1 ? __any_sync(0xffffffffu, !ok) : __syncthreads_or(!ok);
         if (bad) {
             failed = true;
             mma_lost = true;
@@ -538,7 +539,7 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
         if constexpr (T::CL > 1) {
             exchange_wait(kbar, kphase, T::KX_BYTES);  // the partner's K entries; this CTA's own ones
         } else {
-            __syncthreads();  // K complete
+            if (__syncthreads_or(bad)) return false;  // K complete (or an MMA wait gave up in some warp)
         }
 #pragma unroll
         for (int e = 0; e < E; ++e) {
