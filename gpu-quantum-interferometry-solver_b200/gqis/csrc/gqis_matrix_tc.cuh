@@ -477,6 +477,7 @@ __global__ void __launch_bounds__(TcShape<MM>::THREADS, TcShape<MM>::MIN_CTAS) m
         // thread polls and the CTA meets at a barrier.
         const bool ok = (T::CL == 1 || tid == 0) ? (failed || gqtc::mbar_wait_bounded(bar, phase, kMaxPolls)) : true;
         const bool bad = T::CL == 1 ? __any_sync(0xffffffffu, !ok) : __syncthreads_or(!ok);
+        if constexpr (T::CL == 1 && T::NGM < MM::NG) __syncthreads();  // every point's dvs written
         if (bad) {
             failed = true;
             mma_lost = true;

@@ -209,3 +209,20 @@ def test_tensor_core_split_fp16_keeps_entries_far_below_a_terms_largest():
     ref2 = run(2, False)
     assert 1e-8 < float(np.max(np.abs(ref2))) < 1e-3  # fed by the small couplings only
     assert float(np.max(np.abs(run(2, True) - ref2))) <= 1e-2 * float(np.max(np.abs(ref2)))
+
+
+@pytest.mark.gpu
+def test_tensor_core_diagonal_terms_in_the_epilogue():
+    """Three dense drive operators and a diagonal term at N = 20 (padded to 32) need 320 MMA columns,
+    so the tensor-core kernel adds the diagonal term in its epilogue from each point's sums, which
+    all threads form in shared memory while the MMA runs: the map equals the FP64 form to 5e-6."""
+    import gqis
+    from gqis import matrix_form
+    from test_support_calls import epilogue_diagonal_model
+    args, kwargs = epilogue_diagonal_model()
+    mm, _ = matrix_form.compile_matrix_model(*args[:4], sweep_symbols=tuple(kwargs["var_arrays"]))
+    assert (mm.num_dense, mm.num_diag) == (3, 1) and not matrix_form.diag_in_mma(mm)
+    ref = gqis.mesolve_2D(*args, **kwargs, fp64=True, rhs_form="matrix")
+    got = gqis.mesolve_2D(*args, **kwargs, precision="fp32", rhs_form="matrix_tc")
+    assert np.max(np.abs(ref)) > 1e-6
+    assert float(np.max(np.abs(got - ref))) <= 5e-6

@@ -70,6 +70,7 @@ def matrix_calls():
                                          rho0_values=rho0)))
     out += runtime_rate_calls()
     out += wide_range_calls()
+    out += epilogue_diagonal_calls()
     args, kwargs = serving_model(8, 6)  # observable traces through the matrix kernels
     args = args[:4] + (np.linspace(0.0, 5.0, 101),)
     trace = dict(kwargs, return_time_trace=True, time_trace_every=7)
@@ -298,3 +299,34 @@ def wide_range_calls():
         if decay:
             out.append(("mesolve_2D", args, dict(kwargs, precision="fp32", rhs_form="matrix_tc")))
     return out
+
+
+def epilogue_diagonal_model():
+    """(args, kwargs) of a 20-level model (padded to 32) with three dense drive operators and one
+    diagonal term: 2 x 32 rows x 5 terms = 320 MMA columns exceed one MMA, so the tensor-core kernel
+    takes the diagonal term in its epilogue. 4 x 3 (eps, A) points, 300 RK4 steps on [0, 15]."""
+    eps, A, t = sp.symbols("eps A t", real=True)
+    d1, d2, d3 = sp.symbols("Drive1 Drive2 Drive3", real=True)
+    N = 20
+    rng = np.random.default_rng(7)
+
+    def hermitian(scale):
+        G = (rng.normal(size=(N, N)) + 1j * rng.normal(size=(N, N))) * scale / np.sqrt(2 * N)
+        return sp.Matrix(np.round((G + G.conj().T) / 2, 6).tolist())
+    H = hermitian(1.0) + eps * sp.diag(*range(N)) + d1 * hermitian(1.0) + d2 * hermitian(0.5) + d3 * hermitian(0.3)
+    col = []
+    for k in range(1, N):
+        L = sp.zeros(N)
+        L[k - 1, k] = sp.sqrt(0.01)
+        col.append(L)
+    O = sp.zeros(N)
+    O[N - 1, N - 1] = 1
+    drive = {"Drive1": A * sp.cos(t), "Drive2": A * sp.sin(t), "Drive3": A * sp.cos(2 * t)}
+    var = {eps: np.linspace(-0.5, 0.5, 4), A: np.linspace(0.0, 2.0, 3)}
+    return (H, drive, col, O, np.linspace(0.0, 15.0, 301)), {"var_arrays": var}
+
+
+def epilogue_diagonal_calls():
+    args, kwargs = epilogue_diagonal_model()
+    return [("mesolve_2D", args, dict(kwargs, fp64=True, rhs_form="matrix")),
+            ("mesolve_2D", args, dict(kwargs, precision="fp32", rhs_form="matrix_tc"))]
