@@ -438,6 +438,7 @@ def _tensor_core_tables(mm: MatrixModel):
     static constexpr bool kOwnTerms = {'true' if own else 'false'};
     static constexpr bool kJumpsOnDiagonal = {'true' if on_diag else 'false'};
     static constexpr bool kDiagInMma = {'true' if diag_in_mma(mm) else 'false'};
+    static constexpr bool kObsDiagonal = {'true' if not np.any(mm.obs - np.diag(np.diag(mm.obs))) else 'false'};
     static constexpr int TC_CL = {tensor_core_shape(mm)[0]};
     static constexpr int TC_E = {E};
     __device__ __forceinline__ static const int* tcj_count() {{ return mm_tcj_count; }}
