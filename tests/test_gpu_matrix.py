@@ -226,3 +226,19 @@ def test_tensor_core_diagonal_terms_in_the_epilogue():
     got = gqis.mesolve_2D(*args, **kwargs, precision="fp32", rhs_form="matrix_tc")
     assert np.max(np.abs(ref)) > 1e-6
     assert float(np.max(np.abs(got - ref))) <= 5e-6
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("N", [16, 64])
+def test_tensor_core_form_with_an_offdiagonal_observable(N):
+    """An observable with coherences (the kernel's general observable path; a diagonal observable is
+    read only by the threads that hold diagonal elements): the tensor-core map equals the FP64 form
+    to 5e-6, one CTA per tile (N = 16) and on two-CTA clusters (N = 64)."""
+    import gqis
+    from gqis import matrix_form
+    from test_support_calls import offdiagonal_observable_model
+    args, kwargs = offdiagonal_observable_model(N)
+    ref = gqis.mesolve_2D(*args, **kwargs, fp64=True, rhs_form="matrix")
+    got = gqis.mesolve_2D(*args, **kwargs, precision="fp32", rhs_form="matrix_tc")
+    assert np.max(np.abs(ref.imag)) > 1e-6 or np.max(np.abs(ref.real)) > 1e-3  # a non-trivial map
+    assert float(np.max(np.abs(got - ref))) <= 5e-6

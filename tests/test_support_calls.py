@@ -71,6 +71,7 @@ def matrix_calls():
     out += runtime_rate_calls()
     out += wide_range_calls()
     out += epilogue_diagonal_calls()
+    out += offdiagonal_observable_calls()
     args, kwargs = serving_model(8, 6)  # observable traces through the matrix kernels
     args = args[:4] + (np.linspace(0.0, 5.0, 101),)
     trace = dict(kwargs, return_time_trace=True, time_trace_every=7)
@@ -330,3 +331,25 @@ def epilogue_diagonal_calls():
     args, kwargs = epilogue_diagonal_model()
     return [("mesolve_2D", args, dict(kwargs, fp64=True, rhs_form="matrix")),
             ("mesolve_2D", args, dict(kwargs, precision="fp32", rhs_form="matrix_tc"))]
+
+
+def offdiagonal_observable_model(N):
+    """(args, kwargs) of the N-level scaling model on its small test grid with a Hermitian observable
+    that has off-diagonal entries (a coherence between levels 0 and 1, one between N - 2 and N - 1,
+    and a population): the general observable path of the tensor-core kernel."""
+    _, args, kwargs = hilbert_model(N)
+    O = sp.zeros(N)
+    O[0, 1] = O[1, 0] = 1
+    O[N - 2, N - 1] = sp.I / 2
+    O[N - 1, N - 2] = -sp.I / 2
+    O[N - 1, N - 1] = sp.Rational(1, 3)
+    return args[:3] + (O,) + args[4:], kwargs
+
+
+def offdiagonal_observable_calls():
+    out = []
+    for N in (16, 64):
+        args, kwargs = offdiagonal_observable_model(N)
+        out.append(("mesolve_2D", args, dict(kwargs, fp64=True, rhs_form="matrix")))
+        out.append(("mesolve_2D", args, dict(kwargs, precision="fp32", rhs_form="matrix_tc")))
+    return out
