@@ -250,3 +250,12 @@ def test_batch_launch_checks_its_arguments_before_any_cuda_call():
     mlib = ctypes.CDLL(str(path))
     abi.bind_module(mlib)
     assert mlib.gqis_sweep_launch_batch(descs, 1, None, None) == abi.ERR_UNSUPPORTED
+
+
+def test_probe_library_exports_the_fma_and_tensor_core_probes():
+    """The roofline denominators: FMA-pipe probes and the tcgen05 kind::tf32 / kind::f16 MMA probes
+    (loading needs no GPU; nothing is called)."""
+    from gqis import native
+    lib = ctypes.CDLL(str(native.build("gqis_probe")))
+    for name in ("gqis_probe_fma", "gqis_probe_tc_tf32", "gqis_probe_tc_f16"):
+        assert hasattr(lib, name), name

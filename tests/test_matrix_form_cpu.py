@@ -154,3 +154,15 @@ def test_tensor_core_shape_of_the_two_cta_kernel():
     assert matrix_form.tensor_core_blockers(fake(32, 3, 1), "fp32") == []  # 2 x 32 x 4 = 256 columns
     assert "exceed one MMA" in matrix_form.tensor_core_blockers(fake(32, 4, 1), "fp32")[0]
     assert "padded dimension 48" in matrix_form.tensor_core_blockers(fake(48, 1, 1), "fp32")[0]
+
+
+def test_tensor_core_module_flags_a_diagonal_observable():
+    """The tensor-core kernel reads a diagonal observable only in the threads that hold diagonal
+    elements (kObsDiagonal); an observable with coherences takes the general path."""
+    from gqis import workloads
+    w = workloads.n_level(16, side=2)
+    for O, diagonal in ((w["mean_operator"], True), (w["mean_operator"] + sp.Matrix(16, 16, lambda i, j: 1 if abs(i - j) == 1 else 0), False)):
+        mm, _ = matrix_form.compile_matrix_model(w["H"], w["Drive"], w["Col_Ops"], O,
+                                                 sweep_symbols=tuple(w["var_arrays"]), reuse=False)
+        src = matrix_form.module_source(mm, "fp32", "mean", False, tensor_cores=True)
+        assert f"kObsDiagonal = {'true' if diagonal else 'false'};" in src
